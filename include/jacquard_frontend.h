@@ -1,0 +1,96 @@
+/*
+ * jacquard_frontend.h -- host-side script front end (libjq_frontend.so).
+ *
+ * Builds the reference's FlattenedScriptV1 instruction stream from a design:
+ *   design (AIG) -> major stages -> partitions -> boomerang stages -> script.
+ * It takes the place of the reference's Rust front end
+ * (src/sim/setup.rs:75-326 load_design, src/staging.rs, src/repcut.rs,
+ * src/pe.rs, src/flatten.rs), which cannot be built here.  The script it emits
+ * is consumed unchanged by the interpreter entry points in jacquard_b200.h.
+ * Pure host code: no CUDA calls.
+ */
+#ifndef JACQUARD_FRONTEND_H
+#define JACQUARD_FRONTEND_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Seeded synthetic design (aigpdk semantics).  See generate.cpp. */
+typedef struct {
+  uint64_t seed;
+  uint32_t n_clusters;        /* 1 = flat levelized logic */
+  uint32_t nodes_per_cluster; /* AND nodes per cluster */
+  uint32_t depth;             /* logic levels */
+  uint32_t fanin_window;      /* fanins drawn from the previous N levels */
+  double intra_frac;          /* probability a fanin stays in its cluster */
+  uint32_t n_dff, n_pi, n_po, n_sram;
+  uint32_t sram_addr_bits;    /* used address bits of each SRAM (<= 13) */
+  int32_t with_reset;         /* input 0 is a synchronous reset of every DFF */
+} jqf_gen_params;
+
+typedef struct {
+  uint64_t num_pins, num_and, num_dffs, num_pos, num_srams;
+  uint32_t clock_flag_pin, reset_pin;
+} jqf_design_info_t;
+
+#define JQF_SRAM_RECORD_WORDS (13 + 1 + 32 + 13 + 32 + 32)
+
+void *jqf_generate(const jqf_gen_params *p, uint64_t *num_and);
+void jqf_free_design(void *design);
+int jqf_design_info(void *design, jqf_design_info_t *out);
+/* Copy one design array (see capi.cpp for `which`); returns its byte size. */
+int64_t jqf_design_array(void *design, int which, void *dst, size_t cap);
+/* Per-pin gate delays in ps (num_pins + 1 entries each), injected into the
+ * script's padding slots at build time (src/flatten.rs:1812-1846). */
+int jqf_set_delays(void *design, const uint32_t *rise, const uint32_t *fall, size_t n);
+
+typedef struct {
+  size_t num_blocks;           /* CTAs of the interpreter launch */
+  int32_t xprop;               /* classify X-capable partitions, words 8/9 */
+  uint32_t n_level_split;
+  const uint32_t *level_split; /* cumulative global levels (--level-split) */
+  uint32_t target_cone;        /* partitioner: AND nodes per chunk (0 = default) */
+  uint32_t target_endpoint_bits;
+  int32_t num_threads;         /* 0 = all host threads */
+  int32_t merge_passes;
+} jqf_build_params;
+
+typedef struct {
+  uint64_t num_blocks, num_major_stages, blocks_data_len;
+  uint32_t reg_io_state_size, sram_storage_size;
+  uint32_t xprop_enabled, xprop_state_offset;
+  uint64_t num_partitions, num_delay_patches, total_boomerang_stages;
+} jqf_script_info_t;
+
+void *jqf_build_script(void *design, const jqf_build_params *bp, char *err, size_t errlen);
+void jqf_free_script(void *script);
+int jqf_script_info(void *script, jqf_script_info_t *out);
+int64_t jqf_script_array(void *script, int which, void *dst, size_t cap);
+
+/* Host-side script validator (same walk as the kernel). 0 = valid. */
+int jqf_validate(const uint64_t *blocks_start, size_t num_blocks, size_t num_major_stages,
+                 const uint32_t *blocks_data, size_t blocks_data_len,
+                 uint32_t reg_io_state_size, uint32_t sram_storage_size,
+                 size_t state_words, char *err, size_t errlen);
+
+/* Timing constraint buffer, build_timing_constraint_buffer
+ * (src/flatten.rs:1891-1924) with the clock-arrival fold of :97-123. */
+int jqf_constraint_buffer(uint32_t num_words, uint64_t clock_period_ps, size_t n,
+                          const uint16_t *setup_ps, const uint16_t *hold_ps,
+                          const int16_t *clock_arrival_ps, const uint32_t *data_state_pos,
+                          uint32_t *out_clock_ps, uint32_t *out_words);
+
+/* Delay injection on explicit patch arrays (src/flatten.rs:1812-1846). */
+int jqf_inject_delays(uint32_t *blocks_data, size_t blocks_data_len, size_t n_patches,
+                      const uint64_t *offsets, const uint32_t *pins_start, const uint32_t *pins,
+                      const uint16_t *rise, const uint16_t *fall, size_t n_pins);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,206 @@
+// Endpoint partitioner for one major stage.
+//
+// The reference partitions endpoints with a RepCut hypergraph handed to
+// mt-kahypar (src/repcut.rs:58-272, src/sim/setup.rs:520-601), then merges
+// partitions greedily (src/pe.rs:855-1070).  mt-kahypar is a third-party
+// library that is not available here, so this file implements its own
+// locality partitioner with the same contract -- every endpoint lands in
+// exactly one partition whose logic fits the boomerang resources:
+//   1. endpoints are ordered by a breadth-first walk over "shares a shallow
+//      cone gate" adjacency, so endpoints computed from the same logic sit
+//      next to each other;
+//   2. the order is cut into chunks bounded by cone size and endpoint count;
+//   3. each chunk is packed; a chunk that does not fit is split in half and
+//      retried (the reference's halving loop, src/sim/setup.rs:540-580);
+//   4. neighbouring small partitions are merged when the merged one still
+//      packs without more stages (src/pe.rs:855-1070's acceptance rule).
+#include "frontend.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <deque>
+#include <stdexcept>
+#include <thread>
+
+namespace jq {
+
+namespace {
+
+template <class F>
+void parallel_for(size_t n, int threads, F &&f) {
+  if (threads <= 1 || n <= 1) {
+    for (size_t i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> th;
+  for (int t = 0; t < threads; ++t)
+    th.emplace_back([&] {
+      for (;;) {
+        size_t i = next.fetch_add(1);
+        if (i >= n) break;
+        f(i);
+      }
+    });
+  for (auto &t : th) t.join();
+}
+
+}  // namespace
+
+std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
+                                       const PartitionOptions &opt) {
+  const size_t ne = st.num_endpoint_groups();
+  int threads = opt.num_threads > 0 ? opt.num_threads
+                                     : (int)std::max(1u, std::thread::hardware_concurrency());
+  std::vector<Partition> result;
+  if (ne == 0) return result;
+
+  // ---- 1. shallow cone gates per endpoint (depth <= 4, at most 24 gates)
+  const int DEPTH = 4;
+  const size_t CAP = 24;
+  std::vector<std::vector<uint32_t>> shallow(ne);
+  parallel_for(ne, threads, [&](size_t e) {
+    std::vector<std::pair<uint32_t, int>> q;
+    st.for_each_input(g, e, [&](uint32_t p) {
+      if (!st.is_leaf(g, p)) q.push_back({p, 0});
+    });
+    auto &out = shallow[e];
+    for (size_t h = 0; h < q.size() && out.size() < CAP; ++h) {
+      auto [u, d] = q[h];
+      if (std::find(out.begin(), out.end(), u) != out.end()) continue;
+      out.push_back(u);
+      if (d + 1 >= DEPTH) continue;
+      uint32_t a = g.fa[u] >> 1, b = g.fb[u] >> 1;
+      if (!st.is_leaf(g, a)) q.push_back({a, d + 1});
+      if (!st.is_leaf(g, b)) q.push_back({b, d + 1});
+    }
+  });
+  // inverted index gate -> endpoints (skip gates shared too widely)
+  std::unordered_map<uint32_t, std::vector<uint32_t>> inv;
+  inv.reserve(ne * 8);
+  for (size_t e = 0; e < ne; ++e)
+    for (uint32_t u : shallow[e]) {
+      auto &v = inv[u];
+      if (v.size() < 64) v.push_back((uint32_t)e);
+    }
+  // ---- BFS order
+  std::vector<uint32_t> order;
+  order.reserve(ne);
+  std::vector<uint8_t> seen(ne, 0);
+  std::deque<uint32_t> dq;
+  for (size_t s0 = 0; s0 < ne; ++s0) {
+    if (seen[s0]) continue;
+    seen[s0] = 1;
+    dq.push_back((uint32_t)s0);
+    while (!dq.empty()) {
+      uint32_t e = dq.front();
+      dq.pop_front();
+      order.push_back(e);
+      for (uint32_t u : shallow[e]) {
+        auto it = inv.find(u);
+        if (it == inv.end()) continue;
+        for (uint32_t f : it->second)
+          if (!seen[f]) { seen[f] = 1; dq.push_back(f); }
+      }
+    }
+  }
+
+  // ---- 2. chunking by cone size / endpoint bits
+  std::vector<std::vector<uint32_t>> chunks;
+  {
+    std::vector<uint32_t> mark(g.num_pins + 1, 0);
+    uint32_t gen = 1;
+    std::vector<uint32_t> cur;
+    uint64_t cone = 0, bits = 0;
+    std::vector<uint32_t> stk;
+    for (uint32_t e : order) {
+      uint64_t add = 0, eb = 0;
+      stk.clear();
+      st.for_each_input(g, e, [&](uint32_t p) { stk.push_back(p); eb++; });
+      if (!cur.empty() && (bits + eb > opt.target_endpoint_bits)) {
+        chunks.push_back(cur);
+        cur.clear();
+        cone = bits = 0;
+        ++gen;
+      }
+      while (!stk.empty()) {
+        uint32_t u = stk.back();
+        stk.pop_back();
+        if (mark[u] == gen) continue;
+        mark[u] = gen;
+        if (st.is_leaf(g, u)) continue;
+        add++;
+        stk.push_back(g.fa[u] >> 1);
+        stk.push_back(g.fb[u] >> 1);
+      }
+      cur.push_back(e);
+      cone += add;
+      bits += eb;
+      if (cone >= opt.target_cone) {
+        chunks.push_back(cur);
+        cur.clear();
+        cone = bits = 0;
+        ++gen;
+      }
+    }
+    if (!cur.empty()) chunks.push_back(cur);
+  }
+
+  // ---- 3. pack; split failures in half
+  PackOptions po;
+  std::vector<Partition> good;
+  while (!chunks.empty()) {
+    std::vector<Partition> built(chunks.size());
+    std::vector<uint8_t> ok(chunks.size(), 0);
+    parallel_for(chunks.size(), threads, [&](size_t i) {
+      ok[i] = build_partition(g, st, chunks[i], built[i], po);
+    });
+    std::vector<std::vector<uint32_t>> retry;
+    for (size_t i = 0; i < chunks.size(); ++i) {
+      if (ok[i]) {
+        good.push_back(std::move(built[i]));
+        continue;
+      }
+      if (chunks[i].size() == 1)
+        throw std::runtime_error("a single endpoint does not fit one partition; use finer level splits");
+      size_t h = chunks[i].size() / 2;
+      retry.push_back(std::vector<uint32_t>(chunks[i].begin(), chunks[i].begin() + h));
+      retry.push_back(std::vector<uint32_t>(chunks[i].begin() + h, chunks[i].end()));
+    }
+    chunks.swap(retry);
+  }
+
+  // ---- 4. merge neighbours (in endpoint order) when it costs no stages
+  for (int pass = 0; pass < opt.merge_passes && good.size() > 1; ++pass) {
+    std::vector<Partition> merged;
+    // candidate pairs (i, i+1) evaluated in parallel, accepted greedily
+    size_t np = good.size();
+    std::vector<Partition> trial(np);
+    std::vector<uint8_t> tok(np, 0);
+    parallel_for(np - 1, threads, [&](size_t i) {
+      std::vector<uint32_t> eps = good[i].endpoints;
+      eps.insert(eps.end(), good[i + 1].endpoints.begin(), good[i + 1].endpoints.end());
+      Partition p;
+      if (build_partition(g, st, eps, p, po) &&
+          p.stages.size() <= std::max(good[i].stages.size(), good[i + 1].stages.size())) {
+        trial[i] = std::move(p);
+        tok[i] = 1;
+      }
+    });
+    for (size_t i = 0; i < np;) {
+      if (i + 1 < np && tok[i]) {
+        merged.push_back(std::move(trial[i]));
+        i += 2;
+      } else {
+        merged.push_back(std::move(good[i]));
+        i += 1;
+      }
+    }
+    bool changed = merged.size() != good.size();
+    good.swap(merged);
+    if (!changed) break;
+  }
+  return good;
+}
+
+}  // namespace jq
