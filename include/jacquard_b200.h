@@ -1,0 +1,117 @@
+/*
+ * jacquard_b200.h -- C ABI of the B200 (sm_100a) Boolean-processor
+ * interpreter (libjacquard_b200.so).
+ *
+ * Drop-in boundary: the first two symbols have exactly the names, argument
+ * order and meaning of the reference's kernel wrappers in csrc/kernel_v1.cu,
+ * which the reference's Rust side binds through bindgen (build.rs:69) and
+ * calls from sim_cuda (src/bin/jacquard.rs:1135-1147):
+ *   simulate_v1_noninteractive_simple_scan_cuda  <- csrc/kernel_v1.cu:17-46
+ *   simulate_v1_noninteractive_timed_cuda        <- csrc/kernel_v1.cu:49-78
+ * All pointers are caller-owned DEVICE pointers; the launch is asynchronous
+ * on the legacy default stream; like the reference, a launch failure prints
+ * the CUDA error and exits the process (csrc/kernel_v1.cu:6-14).
+ *
+ * The jq_* entry points below have no counterpart symbol in the reference:
+ * they return a status instead of exiting, take an explicit stream, report
+ * barrier timeouts and event-buffer overflow, and add the bit-lane batched
+ * interpreter (many stimulus streams per launch).
+ */
+#ifndef JACQUARD_B200_H
+#define JACQUARD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Reference-compatible entry points (types: usize = size_t, u32, i32, u8). */
+
+/* Runs num_cycles cycles of the script.  states_noninteractive holds
+ * (num_cycles+1) snapshots of state_size u32: snapshot 0 is the initial
+ * state, snapshot c+1 is pre-filled by the caller with edge c+1's inputs and
+ * receives the partitions' outputs.  blocks_start has
+ * num_major_stages*num_blocks+1 entries.  sram_xmask must be a valid device
+ * pointer even when no partition is X-capable.  arrival_state_offset != 0
+ * writes per-word arrival times at that offset of each output snapshot. */
+void simulate_v1_noninteractive_simple_scan_cuda(
+    size_t num_blocks, size_t num_major_stages, const size_t *blocks_start,
+    const uint32_t *blocks_data, uint32_t *sram_data, uint32_t *sram_xmask,
+    size_t num_cycles, size_t state_size, uint32_t *states_noninteractive,
+    int32_t arrival_state_offset);
+
+/* Same, with setup/hold checking.  timing_constraints = [clock_period_ps,
+ * one u32 per state word: setup<<16 | hold]; event_buffer points to the
+ * reference's EventBuffer (csrc/event_buffer.h:45-50: u32 count, u32
+ * overflow, u32 reserved[2], then 1024 events of 8 u32). */
+void simulate_v1_noninteractive_timed_cuda(
+    size_t num_blocks, size_t num_major_stages, const size_t *blocks_start,
+    const uint32_t *blocks_data, uint32_t *sram_data, uint32_t *sram_xmask,
+    size_t num_cycles, size_t state_size, uint32_t *states_noninteractive,
+    const uint32_t *timing_constraints, uint8_t *event_buffer,
+    int32_t arrival_state_offset);
+
+/* ------------------------------------------------------------------------ */
+/* Status-returning interface. */
+
+#define JQ_OK 0
+#define JQ_ERR_INVALID_ARG -1
+#define JQ_ERR_LAUNCH -2          /* CUDA launch / occupancy failure */
+#define JQ_ERR_BARRIER_TIMEOUT -3 /* a grid barrier wait ran out */
+#define JQ_ERR_CUDA -4            /* asynchronous CUDA error */
+#define JQ_ERR_TOO_MANY_BLOCKS -5 /* grid larger than co-resident capacity */
+#define JQ_ERR_EVENT_OVERFLOW 1   /* positive: events were dropped */
+
+/* Event record: identical to the reference's Event (32 bytes). */
+typedef struct {
+  uint32_t event_type, message_id, cycle, reserved;
+  uint32_t data[4];
+} jq_event;
+
+/* Event sink with a caller-chosen capacity (the reference's fixed 1024-slot
+ * EventBuffer is the legacy layout).  `count` counts every event, also those
+ * dropped past `capacity`. */
+typedef struct {
+  uint32_t count, overflow, capacity, reserved;
+  jq_event events[];  /* capacity entries follow */
+} jq_event_buffer;
+
+typedef struct {
+  size_t num_blocks, num_major_stages;
+  const size_t *blocks_start; /* device */
+  const uint32_t *blocks_data; /* device */
+  uint32_t *sram_data, *sram_xmask; /* device; sram_xmask may be NULL */
+  size_t num_cycles, state_size;
+  uint32_t *states; /* device, (num_cycles+1) x state_size */
+  const uint32_t *timing_constraints; /* device or NULL */
+  jq_event_buffer *events; /* device or NULL (required with constraints) */
+  uint32_t event_capacity; /* records that fit in `events` */
+  int32_t arrival_state_offset;
+  uint32_t first_cycle; /* cycle number reported in events */
+  uint64_t barrier_timeout_cycles; /* 0 = default (about a second) */
+  void *stream; /* cudaStream_t, NULL = legacy default stream */
+} jq_sim_args;
+
+/* Plain interpreter (reference layout, one stimulus stream).  Asynchronous;
+ * returns JQ_OK or a launch error.  Kernel-side status (barrier timeout) is
+ * read back with jq_sim_status. */
+int jq_simulate(const jq_sim_args *a);
+
+/* Synchronizes `stream` and returns JQ_OK, JQ_ERR_BARRIER_TIMEOUT or
+ * JQ_ERR_CUDA for the launches made so far on it, and clears the flag. */
+int jq_sim_status(void *stream);
+
+/* Largest grid the plain interpreter can keep co-resident on `device`. */
+int jq_max_blocks(int device, size_t *max_blocks);
+
+/* Human-readable text for a status code. */
+const char *jq_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,443 @@
+// Plain interpreter kernel for sm_100a: the reference's script semantics
+// (csrc/kernel_v1_impl.cuh:32-626), one stimulus stream, persistent over all
+// cycles of a launch with a bounded-wait grid barrier between major stages.
+//
+// Per (cycle, major stage) each CTA walks its partition list:
+//   metadata -> global read (bit gather of state words into 256x32 bits) ->
+//   boomerang stages (16-pair shuffle, 8192->1 AND tree, writeout hooks) ->
+//   SRAM/duplicate permutation + SRAM port -> clock-enable permutation and
+//   DFF commit (+X lanes, +u16 arrivals, +setup/hold events).
+// Script chunks are streamed with 16-byte read-only loads, double-buffered in
+// registers one stage ahead.  State/SRAM reads bypass L1 (written by other
+// SMs between barriers).
+#include "sim_common.cuh"
+
+namespace jqk {
+
+struct PlainParams {
+  unsigned num_blocks, num_major_stages;
+  const size_t *blocks_start;
+  const uint32_t *blocks_data;
+  uint32_t *sram, *sram_x;
+  size_t num_cycles, state_size;
+  uint32_t *states;
+  const uint32_t *constraints;  // [clock, words...] or null
+  jq_event_buffer *events;
+  uint32_t event_cap;
+  int32_t arrival_off;
+  uint32_t first_cycle;
+  uint64_t timeout;
+  int slot;
+};
+
+template <bool TRACK>
+__device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *__restrict__ script,
+                                          const uint32_t *in, uint32_t *out, uint32_t cycle,
+                                          uint32_t *s_meta, uint32_t *s_st, uint32_t *s_stx,
+                                          uint32_t *s_wo, uint32_t *s_wox, uint16_t *s_arr,
+                                          uint16_t *s_woarr) {
+  const int t = threadIdx.x;
+  const uint32_t clock_ps = TRACK && P.constraints ? __ldg(P.constraints) : 0;
+  const uint32_t *cons = P.constraints ? P.constraints + 1 : nullptr;
+  size_t off = 0;
+  for (;;) {
+    s_meta[t] = __ldg(script + off + t);
+    __syncthreads();
+    const uint32_t ns = s_meta[0];
+    if (!ns) break;
+    const uint32_t is_last = s_meta[1], num_ios = s_meta[2], io_off = s_meta[3];
+    const uint32_t num_srams = s_meta[4], sram_off = s_meta[5], R = s_meta[6];
+    const uint32_t num_dup = s_meta[7];
+    const bool is_x = s_meta[8] != 0;
+    const uint32_t xoff = s_meta[9];
+    const uint32_t hw = s_meta[128 + t / 2];
+    const uint32_t hook = (t & 1) ? (hw >> 16) : (hw & 0xffffu);
+    const uint32_t *gr = script + off + 256;
+    const uint32_t *ch = gr + 512 * (size_t)R;
+
+    // prefetch stage 0 (or the SRAM chunk when there are no stages)
+    uint4 c0 = ldg4(ch + 4 * t), c1 = ldg4(ch + 1024 + 4 * t), c2 = ldg4(ch + 2048 + 4 * t),
+          c3 = ldg4(ch + 3072 + 4 * t), cf = ldg4(ch + 4096 + 4 * t);
+
+    // ---- global read
+    uint32_t v = 0, vx = 0;
+    for (uint32_t r = 0; r < R; ++r) {
+      uint2 im = ldg2(gr + 512 * r + 2 * t);
+      uint32_t m = im.y;
+      if (m) {
+        const uint32_t *base = (im.x >> 31) ? out : in;
+        size_t w = im.x & 0x7fffffffu;
+        uint32_t val = ldcg(base + w);
+        uint32_t xv = is_x ? ldcg(base + xoff + w) : 0u;
+        while (m) {
+          uint32_t low = m & (0u - m);
+          v = (v << 1) | ((val & low) ? 1u : 0u);
+          vx = (vx << 1) | ((xv & low) ? 1u : 0u);
+          m ^= low;
+        }
+      }
+    }
+    s_st[t] = v;
+    s_stx[t] = vx;
+    __syncthreads();
+
+    // ---- boomerang stages
+    for (uint32_t bs = 0; bs < ns; ++bs) {
+      const uint32_t *nx = ch + STAGE_WORDS * (bs + 1);
+      uint32_t hin = gather16(s_st, c0, c1, c2, c3);
+      uint32_t hinx = is_x ? gather16(s_stx, c0, c1, c2, c3) : 0u;
+      const uint32_t xa = cf.x, xb = cf.y, ob = cf.z;
+      const uint16_t dly = (uint16_t)(cf.w & 0xffffu);
+      const bool pass = ob == 0xffffffffu;
+      c0 = ldg4(nx + 4 * t);
+      c1 = ldg4(nx + 1024 + 4 * t);
+      c2 = ldg4(nx + 2048 + 4 * t);
+      c3 = ldg4(nx + 3072 + 4 * t);
+      cf = ldg4(nx + 4096 + 4 * t);
+      __syncthreads();
+      s_st[t] = hin;
+      s_stx[t] = hinx;
+      __syncthreads();
+      // level 0: threads 128..255; inputs' arrivals are 0 after the shuffle
+      if (t >= 128) {
+        uint32_t r, rx;
+        xand(s_st[t - 128], s_stx[t - 128], hin, hinx, xa, xb, ob, r, rx);
+        s_st[t] = r;
+        if (is_x) s_stx[t] = rx;
+        if (TRACK) s_arr[t] = dly;
+      } else if (TRACK) {
+        s_arr[t] = 0;
+      }
+      __syncthreads();
+      // levels 1..3 in shared memory
+#pragma unroll
+      for (int hi = 1; hi <= 3; ++hi) {
+        const int w = 1 << (7 - hi);
+        if (t >= w && t < 2 * w) {
+          uint32_t r, rx;
+          xand(s_st[t + w], s_stx[t + w], s_st[t + 2 * w], s_stx[t + 2 * w], xa, xb, ob, r, rx);
+          s_st[t] = r;
+          if (is_x) s_stx[t] = rx;
+          if (TRACK) s_arr[t] = arr_step(pass, s_arr[t + w], s_arr[t + 2 * w], dly);
+        }
+        __syncthreads();
+      }
+      // levels 4..7 inside warp 0, levels 8..12 bit-level in thread 0
+      if (t < 32) {
+        uint32_t cur = s_st[t], curx = s_stx[t];
+        uint32_t ca = TRACK ? (uint32_t)s_arr[t] : 0u;
+        if (t < 16) ca = 0;  // only lanes 16..31 carry level-3 arrivals
+#pragma unroll
+        for (int hi = 4; hi <= 7; ++hi) {
+          const int w = 1 << (7 - hi);
+          uint32_t a = __shfl_down_sync(0xffffffffu, cur, w);
+          uint32_t b = __shfl_down_sync(0xffffffffu, cur, 2 * w);
+          uint32_t ax = __shfl_down_sync(0xffffffffu, curx, w);
+          uint32_t bx = __shfl_down_sync(0xffffffffu, curx, 2 * w);
+          uint32_t aa = __shfl_down_sync(0xffffffffu, ca, w);
+          uint32_t ba = __shfl_down_sync(0xffffffffu, ca, 2 * w);
+          if (t >= w && t < 2 * w) {
+            uint32_t r, rx;
+            xand(a, ax, b, bx, xa, xb, ob, r, rx);
+            cur = r;
+            if (is_x) curx = rx;
+            ca = arr_step(pass, (uint16_t)aa, (uint16_t)ba, dly);
+          }
+        }
+        uint32_t v1 = __shfl_down_sync(0xffffffffu, cur, 1);
+        uint32_t v1x = __shfl_down_sync(0xffffffffu, curx, 1);
+        if (t == 0) {
+          uint32_t r8 = ((v1 << 16) ^ xa) & ((v1 ^ xb) | ob) & 0xffff0000u;
+          uint32_t r9 = ((r8 >> 8) ^ xa) & (((r8 >> 16) ^ xb) | ob) & 0xff00u;
+          uint32_t r10 = ((r9 >> 4) ^ xa) & (((r9 >> 8) ^ xb) | ob) & 0xf0u;
+          uint32_t r11 = ((r10 >> 2) ^ xa) & (((r10 >> 4) ^ xb) | ob) & 0xcu;
+          uint32_t r12 = ((r11 >> 1) ^ xa) & (((r11 >> 2) ^ xb) | ob) & 0x2u;
+          cur = r8 | r9 | r10 | r11 | r12;
+          if (is_x) {
+            uint32_t d, x8, x9, x10, x11, x12;
+            xand(v1 << 16, v1x << 16, v1, v1x, xa, xb, ob, d, x8);
+            x8 &= 0xffff0000u;
+            xand(r8 >> 8, x8 >> 8, r8 >> 16, x8 >> 16, xa, xb, ob, d, x9);
+            x9 &= 0xff00u;
+            xand(r9 >> 4, x9 >> 4, r9 >> 8, x9 >> 8, xa, xb, ob, d, x10);
+            x10 &= 0xf0u;
+            xand(r10 >> 2, x10 >> 2, r10 >> 4, x10 >> 4, xa, xb, ob, d, x11);
+            x11 &= 0xcu;
+            xand(r11 >> 1, x11 >> 1, r11 >> 2, x11 >> 2, xa, xb, ob, d, x12);
+            x12 &= 0x2u;
+            curx = x8 | x9 | x10 | x11 | x12;
+          } else {
+            curx = 0;
+          }
+          ca = 0;  // thread 0's arrival is never advanced
+        }
+        s_st[t] = cur;
+        s_stx[t] = curx;
+        if (TRACK) s_arr[t] = (uint16_t)ca;
+      }
+      __syncthreads();
+      if ((hook >> 8) == bs) {
+        const uint32_t src = hook & 255u;
+        s_wo[t] = s_st[src];
+        if (is_x) s_wox[t] = s_stx[src];
+        if (TRACK) s_woarr[t] = s_arr[src];
+      }
+    }
+    __syncthreads();
+
+    // ---- SRAM & duplicate permutation (c* hold the SRAM chunk now)
+    uint32_t sd = (gather16(s_wo, c0, c1, c2, c3) & ~cf.y) ^ cf.x;
+    uint32_t sdx = is_x ? (gather16(s_wox, c0, c1, c2, c3) & ~cf.y) : 0u;
+    {
+      const uint32_t *ck = ch + STAGE_WORDS * (ns + 1);
+      c0 = ldg4(ck + 4 * t);
+      c1 = ldg4(ck + 1024 + 4 * t);
+      c2 = ldg4(ck + 2048 + 4 * t);
+      c3 = ldg4(ck + 3072 + 4 * t);
+      cf = ldg4(ck + 4096 + 4 * t);
+    }
+    __syncthreads();  // every thread has gathered from s_wo before SRAM/dup slots change
+    const uint32_t en = __shfl_down_sync(0xffffffffu, sd, 1);
+    const uint32_t data = __shfl_down_sync(0xffffffffu, sd, 2);
+    const uint32_t datax = __shfl_down_sync(0xffffffffu, sdx, 2);
+    if ((uint32_t)t < num_srams * 4 && (t & 3) == 0) {
+      const uint32_t i = t >> 2;
+      uint32_t *ram = P.sram + sram_off + (size_t)i * SRAM_WORDS;
+      const uint32_t ra = sd & 0xffffu, wa = sd >> 16;
+      uint32_t r = ldcg(ram + ra), w0 = ldcg(ram + wa);
+      uint32_t rx = 0, w0x = 0;
+      const bool hx = is_x && P.sram_x != nullptr;
+      uint32_t *ramx = hx ? P.sram_x + sram_off + (size_t)i * SRAM_WORDS : nullptr;
+      if (hx) {
+        rx = ldcg(ramx + ra);
+        w0x = ldcg(ramx + wa);
+      }
+      s_wo[num_ios - num_srams + i] = r;
+      ram[wa] = (w0 & ~en) | (data & en);
+      if (is_x) {
+        s_wox[num_ios - num_srams + i] = rx;
+        if (hx) ramx[wa] = (w0x & ~en) | (datax & en);
+      }
+    } else if ((uint32_t)t >= num_srams * 4 && (uint32_t)t < num_srams * 4 + num_dup) {
+      const uint32_t slot = num_ios - num_srams - num_dup + (t - num_srams * 4);
+      s_wo[slot] = sd;
+      if (is_x) s_wox[slot] = sdx;
+    }
+    __syncthreads();
+
+    // ---- clock-enable permutation and commit
+    uint32_t cp = (gather16(s_wo, c0, c1, c2, c3) & ~cf.y) ^ cf.x;
+    uint32_t cpx = is_x ? (gather16(s_wox, c0, c1, c2, c3) & ~cf.y) : 0u;
+    if ((uint32_t)t < num_ios) {
+      const size_t o = (size_t)io_off + t;
+      const uint32_t wv = s_wo[t] ^ cf.z;
+      const uint32_t old = ldcg(in + o);
+      out[o] = (old & ~cp) | (wv & cp);
+      if (is_x) {
+        const uint32_t oldx = ldcg(in + xoff + o);
+        const uint32_t wx = s_wox[t];
+        out[xoff + o] = (oldx & ~cp & ~cpx) | (wx & cp & ~cpx) | cpx;
+      }
+      if (TRACK) {
+        const uint16_t a = s_woarr[t];
+        if (P.arrival_off != 0) out[(size_t)(uint32_t)P.arrival_off + o] = (uint32_t)a;
+        if (cons != nullptr && cp != 0) {
+          const uint32_t c = __ldg(cons + o);
+          if (c != 0) {
+            const uint16_t su = (uint16_t)(c >> 16), ho = (uint16_t)(c & 0xffffu);
+            if (a > 0 && (uint32_t)a + (uint32_t)su > clock_ps)
+              push_event(P.events, P.event_cap, 4, (uint32_t)o, cycle,
+                         (uint32_t)((int32_t)clock_ps - (int32_t)a - (int32_t)su), a, su);
+            if (a < ho)
+              push_event(P.events, P.event_cap, 5, (uint32_t)o, cycle,
+                         (uint32_t)((int32_t)a - (int32_t)ho), a, ho);
+          }
+        }
+      }
+    }
+    off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    if (is_last) break;
+    __syncthreads();
+  }
+}
+
+template <bool TRACK>
+__global__ void __launch_bounds__(NT, 3) jq_plain_kernel(PlainParams P) {
+  __shared__ uint32_t s_meta[NT], s_st[NT], s_stx[NT], s_wo[NT], s_wox[NT];
+  __shared__ uint16_t s_arr[NT], s_woarr[NT];
+  __shared__ size_t s_start[32];
+  const int t = threadIdx.x;
+  s_wo[t] = 0;
+  s_wox[t] = 0;
+  s_stx[t] = 0;
+  s_arr[t] = 0;
+  s_woarr[t] = 0;
+  if (t < (int)P.num_major_stages) s_start[t] = P.blocks_start[(size_t)t * P.num_blocks + blockIdx.x];
+  __syncthreads();
+  for (size_t c = 0; c < P.num_cycles; ++c) {
+    const uint32_t *in = P.states + c * P.state_size;
+    uint32_t *out = P.states + (c + 1) * P.state_size;
+    for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
+      run_block<TRACK>(P, P.blocks_data + s_start[ms], in, out, P.first_cycle + (uint32_t)c,
+                       s_meta, s_st, s_stx, s_wo, s_wox, s_arr, s_woarr);
+      if (!grid_barrier(P.slot, P.num_blocks, P.timeout)) return;
+    }
+  }
+}
+
+}  // namespace jqk
+
+// ------------------------------------------------------------------ host side
+#include <cstdio>
+#include <cstdlib>
+
+using namespace jqk;
+
+namespace {
+
+int g_max_blocks_cache[64];
+
+int launch_plain(const jq_sim_args *a, uint32_t event_cap, int slot) {
+  if (!a || a->num_blocks == 0 || a->num_major_stages == 0 || a->num_major_stages > 32 ||
+      !a->blocks_start || !a->blocks_data || !a->states)
+    return JQ_ERR_INVALID_ARG;
+  if (a->timing_constraints && !a->events) return JQ_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)a->stream;
+  const bool track = a->arrival_state_offset != 0 || a->timing_constraints != nullptr;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  size_t maxb = 0;
+  if (jq_max_blocks(dev, &maxb) != JQ_OK) return JQ_ERR_LAUNCH;
+  if (a->num_blocks > maxb) return JQ_ERR_TOO_MANY_BLOCKS;
+  PlainParams P;
+  P.num_blocks = (unsigned)a->num_blocks;
+  P.num_major_stages = (unsigned)a->num_major_stages;
+  P.blocks_start = a->blocks_start;
+  P.blocks_data = a->blocks_data;
+  P.sram = a->sram_data;
+  P.sram_x = a->sram_xmask;
+  P.num_cycles = a->num_cycles;
+  P.state_size = a->state_size;
+  P.states = a->states;
+  P.constraints = a->timing_constraints;
+  P.events = a->events;
+  P.event_cap = event_cap;
+  P.arrival_off = a->arrival_state_offset;
+  P.first_cycle = a->first_cycle;
+  P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
+  P.slot = slot;
+  // reset this slot's barrier (ordered before the kernel on the stream)
+  static const unsigned zero_u[1] = {0};
+  static const int zero_i[1] = {0};
+  if (cudaMemcpyToSymbolAsync(g_bar_count, zero_u, sizeof(unsigned), slot * sizeof(unsigned),
+                              cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return JQ_ERR_LAUNCH;
+  if (cudaMemcpyToSymbolAsync(g_status, zero_i, sizeof(int), slot * sizeof(int),
+                              cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return JQ_ERR_LAUNCH;
+  void *args[] = {&P};
+  cudaError_t e = track ? cudaLaunchCooperativeKernel((void *)jq_plain_kernel<true>, P.num_blocks,
+                                                      NT, args, 0, st)
+                        : cudaLaunchCooperativeKernel((void *)jq_plain_kernel<false>, P.num_blocks,
+                                                      NT, args, 0, st);
+  return e == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
+}
+
+void die_on(int rc, const char *what) {
+  if (rc == JQ_OK) return;
+  cudaError_t e = cudaGetLastError();
+  printf("CUDA error at %s: %s (%s)\n", what, jq_strerror(rc), cudaGetErrorString(e));
+  exit(EXIT_FAILURE);
+}
+
+}  // namespace
+
+extern "C" {
+
+int jq_max_blocks(int device, size_t *max_blocks) {
+  if (device < 0 || device >= 64 || !max_blocks) return JQ_ERR_INVALID_ARG;
+  if (!g_max_blocks_cache[device]) {
+    int sms = 0, a = 0, b = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+      return JQ_ERR_LAUNCH;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, jq_plain_kernel<true>, NT, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, jq_plain_kernel<false>, NT, 0) != cudaSuccess)
+      return JQ_ERR_LAUNCH;
+    g_max_blocks_cache[device] = sms * (a < b ? a : b);
+  }
+  *max_blocks = (size_t)g_max_blocks_cache[device];
+  return JQ_OK;
+}
+
+int jq_simulate(const jq_sim_args *a) {
+  return launch_plain(a, a ? a->event_capacity : 0, 0);
+}
+
+int jq_sim_status(void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return JQ_ERR_CUDA;
+  int flags[1] = {0};
+  if (cudaMemcpyFromSymbol(flags, g_status, sizeof(int), 0) != cudaSuccess) return JQ_ERR_CUDA;
+  static const int zero_i[1] = {0};
+  cudaMemcpyToSymbol(g_status, zero_i, sizeof(int), 0);
+  return flags[0];
+}
+
+const char *jq_strerror(int code) {
+  switch (code) {
+    case JQ_OK: return "ok";
+    case JQ_ERR_INVALID_ARG: return "invalid argument";
+    case JQ_ERR_LAUNCH: return "kernel launch failed";
+    case JQ_ERR_BARRIER_TIMEOUT: return "grid barrier wait timed out";
+    case JQ_ERR_CUDA: return "CUDA error";
+    case JQ_ERR_TOO_MANY_BLOCKS: return "more blocks than can be co-resident";
+    case JQ_ERR_EVENT_OVERFLOW: return "event buffer overflowed";
+    default: return "unknown status";
+  }
+}
+
+void simulate_v1_noninteractive_simple_scan_cuda(size_t num_blocks, size_t num_major_stages,
+                                                 const size_t *blocks_start,
+                                                 const uint32_t *blocks_data, uint32_t *sram_data,
+                                                 uint32_t *sram_xmask, size_t num_cycles,
+                                                 size_t state_size, uint32_t *states_noninteractive,
+                                                 int32_t arrival_state_offset) {
+  jq_sim_args a = {};
+  a.num_blocks = num_blocks;
+  a.num_major_stages = num_major_stages;
+  a.blocks_start = blocks_start;
+  a.blocks_data = blocks_data;
+  a.sram_data = sram_data;
+  a.sram_xmask = sram_xmask;
+  a.num_cycles = num_cycles;
+  a.state_size = state_size;
+  a.states = states_noninteractive;
+  a.arrival_state_offset = arrival_state_offset;
+  die_on(launch_plain(&a, 0, 0), "simulate_v1_noninteractive_simple_scan_cuda");
+}
+
+void simulate_v1_noninteractive_timed_cuda(size_t num_blocks, size_t num_major_stages,
+                                           const size_t *blocks_start, const uint32_t *blocks_data,
+                                           uint32_t *sram_data, uint32_t *sram_xmask,
+                                           size_t num_cycles, size_t state_size,
+                                           uint32_t *states_noninteractive,
+                                           const uint32_t *timing_constraints,
+                                           uint8_t *event_buffer, int32_t arrival_state_offset) {
+  jq_sim_args a = {};
+  a.num_blocks = num_blocks;
+  a.num_major_stages = num_major_stages;
+  a.blocks_start = blocks_start;
+  a.blocks_data = blocks_data;
+  a.sram_data = sram_data;
+  a.sram_xmask = sram_xmask;
+  a.num_cycles = num_cycles;
+  a.state_size = state_size;
+  a.states = states_noninteractive;
+  a.timing_constraints = timing_constraints;
+  a.events = (jq_event_buffer *)event_buffer;
+  a.arrival_state_offset = arrival_state_offset;
+  // the reference's EventBuffer holds MAX_EVENTS = 1024 records
+  die_on(launch_plain(&a, 1024, 0), "simulate_v1_noninteractive_timed_cuda");
+}
+
+}  // extern "C"

@@ -63,6 +63,14 @@ def _lib():
         lib.jqf_script_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(_ScriptInfo)]
         lib.jqf_script_array.restype = ctypes.c_int64
         lib.jqf_script_array.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+        vp, sz, u32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32
+        lib.jqf_validate.restype = ctypes.c_int
+        lib.jqf_validate.argtypes = [vp, sz, sz, vp, sz, u32, u32, sz, ctypes.c_char_p, sz]
+        lib.jqf_constraint_buffer.restype = ctypes.c_int
+        lib.jqf_constraint_buffer.argtypes = [u32, ctypes.c_uint64, sz, vp, vp, vp, vp,
+                                              ctypes.POINTER(u32), vp]
+        lib.jqf_inject_delays.restype = ctypes.c_int
+        lib.jqf_inject_delays.argtypes = [vp, sz, sz, vp, vp, vp, vp, vp, sz]
         lib._jq_typed = True
     return lib
 

@@ -1,0 +1,76 @@
+"""Seeded test designs / scripts / stimulus shared by the tests."""
+import functools
+
+import numpy as np
+
+from jacquard_b200 import frontend, state
+
+
+@functools.lru_cache(maxsize=None)
+def design(kind, seed=11):
+    if kind == "tiny":
+        p = frontend.DesignParams(seed=seed, nodes_per_cluster=1500, depth=10, n_dff=96,
+                                  n_pi=12, n_po=10)
+    elif kind == "small":
+        p = frontend.small_params(seed=1)
+    elif kind == "sram":
+        p = frontend.DesignParams(seed=seed, n_clusters=4, nodes_per_cluster=1200, depth=16,
+                                  intra_frac=0.9, n_dff=400, n_pi=24, n_po=16, n_sram=3,
+                                  sram_addr_bits=6, with_reset=1)
+    elif kind == "soc_mini":
+        p = frontend.soc_params(seed=2, n_clusters=8, n_dff=3000, n_sram=2)
+    else:
+        raise KeyError(kind)
+    return frontend.Design(p)
+
+
+@functools.lru_cache(maxsize=None)
+def script(kind, num_blocks, split=(), xprop=False, timing_seed=0):
+    d = design(kind)
+    if timing_seed:
+        rng = np.random.default_rng(timing_seed)
+        n = d.num_pins + 1
+        kinds = d.kind
+        r = rng.integers(20, 201, size=n).astype(np.uint32)
+        r[kinds != 1] = 0
+        d.set_delays(r, r)
+    s = d.build_script(num_blocks=num_blocks, level_split=split, xprop=xprop)
+    if timing_seed:
+        d.set_delays(np.zeros(d.num_pins + 1, np.uint32), np.zeros(d.num_pins + 1, np.uint32))
+    return s
+
+
+def stimulus(kind, s, cycles, seed=3, p_toggle=0.5, reset_cycles=2, x_init=False):
+    """Snapshot buffer (cycles+1, effective) for script s of design kind."""
+    d = design(kind)
+    v = state.random_stimulus_states(s, d, cycles, seed, p_toggle, reset_cycles)
+    if s.xprop_enabled:
+        v = state.expand_states_for_xprop(v, s)
+        if not x_init:
+            v[0, s.reg_io_state_size:] = 0  # known initial state
+    if s.timing_arrivals_enabled:
+        v = state.expand_states_for_arrivals(v, s)
+    return np.ascontiguousarray(v)
+
+
+def constraint_buffer(kind, s, clock_ps=10_000, setup=30, hold=10, seed=5):
+    """[clock, per-word setup<<16|hold] with per-DFF clock arrival U[0,300]."""
+    import ctypes
+    from jacquard_b200._native import load
+    d = design(kind)
+    rng = np.random.default_rng(seed)
+    n = int(d.num_dffs)
+    su = np.full(n, setup, np.uint16)
+    ho = np.full(n, hold, np.uint16)
+    ca = rng.integers(0, 301, size=n).astype(np.int16)
+    pos = np.ascontiguousarray(s.dff_data_pos, dtype=np.uint32)
+    out = np.zeros(s.reg_io_state_size, np.uint32)
+    clk = ctypes.c_uint32()
+    from jacquard_b200.frontend import _lib
+    L = _lib()
+    L.jqf_constraint_buffer(ctypes.c_uint32(s.reg_io_state_size), ctypes.c_uint64(clock_ps),
+                            ctypes.c_size_t(n), su.ctypes.data_as(ctypes.c_void_p),
+                            ho.ctypes.data_as(ctypes.c_void_p), ca.ctypes.data_as(ctypes.c_void_p),
+                            pos.ctypes.data_as(ctypes.c_void_p), ctypes.byref(clk),
+                            out.ctypes.data_as(ctypes.c_void_p))
+    return np.concatenate([[np.uint32(clk.value)], out]).astype(np.uint32)

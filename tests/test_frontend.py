@@ -1,0 +1,107 @@
+"""Front end: scripts are valid, and the oracle running a script computes the
+same DFF states and outputs as a gate-level simulation of the design."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import cases
+import oracle_lib
+from jacquard_b200 import state
+from jacquard_b200._native import load
+
+
+def netlist_check(kind, s, cycles=24, seed=3):
+    d = cases.design(kind)
+    vals = state.stimulus_inputs(s, d, cycles, seed, 0.5, 2)
+    st = state.pack_inputs(s, vals).reshape(-1).copy()
+    oracle_lib.simulate(s, st, cycles, s.reg_io_state_size)
+    st = st.reshape(cycles + 1, -1)
+    dpos = state.dff_positions(s, d)
+    dff0 = state.bits_at(st[:1], dpos)[0]
+    dff, pov = oracle_lib.aig_simulate(d, s.input_layout, vals, dff0, cycles)
+    assert np.array_equal(state.bits_at(st, dpos), dff)
+    assert np.array_equal(state.bits_at(st[1:], state.po_positions(s, d)), pov[1:])
+
+
+@pytest.mark.parametrize("kind,nb,split", [
+    ("tiny", 1, ()), ("tiny", 4, ()), ("tiny", 148, (5,)), ("tiny", 7, (3, 6, 9)),
+    ("small", 64, (8, 16, 24)), ("sram", 16, (8,)), ("sram", 3, ()),
+])
+def test_script_computes_the_design(kind, nb, split):
+    netlist_check(kind, cases.script(kind, nb, split))
+
+
+def test_soc_like_design_with_major_stages():
+    netlist_check("soc_mini", cases.script("soc_mini", 148, (20, 40, 60)), cycles=12)
+
+
+def validate(s, words=None, data=None, rio=None):
+    from jacquard_b200.frontend import _lib
+    L = _lib()
+    bs = np.ascontiguousarray(s.blocks_start, np.uint64)
+    bd = np.ascontiguousarray(s.blocks_data if data is None else data, np.uint32)
+    err = ctypes.create_string_buffer(256)
+    vp = ctypes.c_void_p
+    r = L.jqf_validate(vp(bs.ctypes.data), ctypes.c_size_t(s.num_blocks), ctypes.c_size_t(s.num_major_stages),
+                       vp(bd.ctypes.data), ctypes.c_size_t(bd.size),
+                       ctypes.c_uint32(s.reg_io_state_size if rio is None else rio),
+                       ctypes.c_uint32(s.sram_storage_size),
+                       ctypes.c_size_t(words or s.reg_io_state_size), err, 256)
+    return r, err.value.decode()
+
+
+def test_validator_accepts_built_scripts_and_rejects_corruption():
+    s = cases.script("sram", 16, (8,))
+    assert validate(s) == (0, "")
+    # global-read index past the state
+    bad = s.blocks_data.copy()
+    first = int(s.blocks_start[0])
+    while bad[first] == 0:
+        first += 256
+    R = int(bad[first + 6])
+    assert R > 0
+    t = int(np.nonzero(bad[first + 256 + 1:first + 256 + 512:2])[0][0])
+    bad[first + 256 + 2 * t] = s.reg_io_state_size + 5
+    assert validate(s, data=bad)[0] != 0
+    # shuffle index past the 8192 bits
+    bad = s.blocks_data.copy()
+    bad[first + 256 + 512 * R] = 9000
+    assert validate(s, data=bad)[0] != 0
+    # IO range past the state
+    assert validate(s, rio=1)[0] != 0
+
+
+def test_xprop_classification_marks_partitions():
+    s = cases.script("sram", 16, (8,), xprop=True)
+    assert s.partition_x_capable.any()
+    assert s.xprop_state_offset == s.reg_io_state_size
+    bd = s.blocks_data
+    for stage in range(s.num_major_stages):
+        for b in range(s.num_blocks):
+            off = int(s.blocks_start[stage * s.num_blocks + b])
+            if bd[off] == 0:
+                continue
+            assert bd[off + 9] == s.reg_io_state_size
+
+
+def test_timing_delays_are_injected():
+    s = cases.script("sram", 16, (8,), timing_seed=9)
+    # every boomerang flag chunk padding word holds a delay in [0, 65535]
+    bd = s.blocks_data
+    seen = 0
+    for stage in range(s.num_major_stages):
+        for b in range(s.num_blocks):
+            off = int(s.blocks_start[stage * s.num_blocks + b])
+            while bd[off]:
+                ns, R = int(bd[off]), int(bd[off + 6])
+                ch = off + 256 + 512 * R
+                for k in range(ns):
+                    pad = bd[ch + 5120 * k + 4096 + 3: ch + 5120 * k + 5120: 4]
+                    seen += int((pad > 0).sum())
+                    assert (pad <= 65535).all()
+                last = bd[off + 1]
+                off = ch + 5120 * (ns + 2)
+                if last:
+                    break
+    assert seen > 0

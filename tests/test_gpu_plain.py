@@ -1,0 +1,135 @@
+"""Plain interpreter on the GPU vs the CPU oracle (bit-exact), through the
+C ABI; the reference's own kernel on the same buffers where it was built."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import cases
+import oracle_lib
+from jacquard_b200 import sim
+
+pytestmark = pytest.mark.gpu
+
+REF_SO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "oracle", "_ref", "libref_kernel.so")
+
+
+def run_gpu(s, states, cycles, sram_init=None, sram_x_init=None, constraints=None, cap=0,
+            arrival_off=0, legacy=False):
+    ds = sim.DeviceScript(s)
+    st = sim.u32_to_dev(states.reshape(-1))
+    n_sram = max(1, s.sram_storage_size)
+    sram = sim.u32_to_dev(sram_init if sram_init is not None else np.zeros(n_sram, np.uint32))
+    sram_x = sim.u32_to_dev(sram_x_init if sram_x_init is not None else np.full(n_sram, 0xFFFFFFFF, np.uint32))
+    cons = sim.u32_to_dev(constraints) if constraints is not None else None
+    ev = sim.new_event_buffer(cap) if cons is not None else None
+    if legacy:
+        L = sim.lib()
+        if cons is None:
+            L.simulate_v1_noninteractive_simple_scan_cuda(
+                s.num_blocks, s.num_major_stages, ds.blocks_start.data_ptr(),
+                ds.blocks_data.data_ptr(), sram.data_ptr(), sram_x.data_ptr(), cycles,
+                states.shape[1], st.data_ptr(), arrival_off)
+        else:
+            L.simulate_v1_noninteractive_timed_cuda(
+                s.num_blocks, s.num_major_stages, ds.blocks_start.data_ptr(),
+                ds.blocks_data.data_ptr(), sram.data_ptr(), sram_x.data_ptr(), cycles,
+                states.shape[1], st.data_ptr(), cons.data_ptr(), ev.data_ptr(), arrival_off)
+        torch.cuda.synchronize()
+    else:
+        sim.simulate(ds, st, cycles, states.shape[1], sram, sram_x, constraints=cons, events=ev,
+                     event_capacity=cap, arrival_state_offset=arrival_off)
+        assert sim.status() == 0
+    out = sim.dev_to_u32(st).reshape(states.shape)
+    evs = sim.read_events(ev) if ev is not None else None
+    return out, sim.dev_to_u32(sram), sim.dev_to_u32(sram_x), evs
+
+
+def run_oracle(s, states, cycles, sram_x_init=True, constraints=None, cap=0, arrival_off=0):
+    st = states.reshape(-1).copy()
+    n_sram = max(1, s.sram_storage_size)
+    sram = np.zeros(n_sram, np.uint32)
+    sram_x = np.full(n_sram, 0xFFFFFFFF, np.uint32) if sram_x_init else None
+    ev, cnt = oracle_lib.simulate(s, st, cycles, states.shape[1], sram=sram, sram_x=sram_x,
+                                  constraints=constraints, event_cap=cap,
+                                  arrival_state_offset=arrival_off)
+    return st.reshape(states.shape), sram, sram_x, (ev, cnt)
+
+
+def sorted_events(rows):
+    return sorted(map(tuple, np.asarray(rows, dtype=np.uint32).reshape(-1, 8).tolist()))
+
+
+@pytest.mark.parametrize("kind,nb,split", [("tiny", 4, ()), ("tiny", 148, (5,)),
+                                           ("small", 64, (8, 16, 24)), ("sram", 16, (8,))])
+def test_plain_two_state_matches_oracle(kind, nb, split):
+    s = cases.script(kind, nb, split)
+    states = cases.stimulus(kind, s, 40)
+    want, wsram, _, _ = run_oracle(s, states, 40)
+    got, gsram, _, _ = run_gpu(s, states, 40)
+    assert np.array_equal(got, want)
+    assert np.array_equal(gsram[:wsram.size], wsram)
+
+
+@pytest.mark.parametrize("kind,nb,split", [("tiny", 8, (5,)), ("sram", 16, (8,))])
+def test_plain_xprop_matches_oracle(kind, nb, split):
+    s = cases.script(kind, nb, split, xprop=True)
+    states = cases.stimulus(kind, s, 32, x_init=True)
+    want, wsram, wsx, _ = run_oracle(s, states, 32)
+    got, gsram, gsx, _ = run_gpu(s, states, 32)
+    assert np.array_equal(got, want)
+    assert np.array_equal(gsram[:wsram.size], wsram)
+    assert np.array_equal(gsx[:wsx.size], wsx)
+
+
+def test_plain_timing_events_and_arrivals_match_oracle():
+    s = cases.script("sram", 16, (8,), timing_seed=9)
+    s.enable_timing_arrivals()
+    states = cases.stimulus("sram", s, 24)
+    cons = cases.constraint_buffer("sram", s, clock_ps=300, setup=30, hold=60)
+    want, _, _, (wev, wcnt) = run_oracle(s, states, 24, constraints=cons, cap=1 << 16,
+                                         arrival_off=s.arrival_state_offset)
+    got, _, _, (gev, gcnt, gov) = run_gpu(s, states, 24, constraints=cons, cap=1 << 16,
+                                          arrival_off=s.arrival_state_offset)
+    s.timing_arrivals_enabled = False
+    s.arrival_state_offset = 0
+    assert np.array_equal(got, want)
+    assert gcnt == wcnt and gcnt > 0
+    assert sorted_events(gev) == sorted_events(wev.view(np.uint32))
+
+
+def test_legacy_symbol_matches_status_entry_point():
+    s = cases.script("tiny", 8, (5,))
+    states = cases.stimulus("tiny", s, 20)
+    a, _, _, _ = run_gpu(s, states, 20)
+    b, _, _, _ = run_gpu(s, states, 20, legacy=True)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference kernel not built")
+@pytest.mark.parametrize("xprop", [False, True])
+def test_reference_kernel_matches_oracle(xprop):
+    """The reference's own CUDA kernel (built from its sources) on the same
+    script and buffers: pins the oracle to the reference itself."""
+    kind = "sram"
+    s = cases.script(kind, 16, (8,), xprop=xprop)
+    states = cases.stimulus(kind, s, 24, x_init=xprop)
+    want, wsram, _, _ = run_oracle(s, states, 24)
+    L = ctypes.CDLL(REF_SO)
+    sz, vp = ctypes.c_size_t, ctypes.c_void_p
+    L.simulate_v1_noninteractive_simple_scan_cuda.argtypes = [sz, sz, vp, vp, vp, vp, sz, sz, vp, ctypes.c_int32]
+    ds = sim.DeviceScript(s)
+    st = sim.u32_to_dev(states.reshape(-1))
+    sram = torch.zeros(max(1, s.sram_storage_size), dtype=torch.int32, device="cuda")
+    sram_x = torch.full((max(1, s.sram_storage_size),), -1, dtype=torch.int32, device="cuda")
+    L.simulate_v1_noninteractive_simple_scan_cuda(s.num_blocks, s.num_major_stages,
+                                                  ds.blocks_start.data_ptr(), ds.blocks_data.data_ptr(),
+                                                  sram.data_ptr(), sram_x.data_ptr(), 24,
+                                                  states.shape[1], st.data_ptr(), 0)
+    torch.cuda.synchronize()
+    got = sim.dev_to_u32(st).reshape(states.shape)
+    assert np.array_equal(got, want)
+    assert np.array_equal(sim.dev_to_u32(sram)[:wsram.size], wsram)
