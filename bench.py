@@ -1,0 +1,318 @@
+"""Benchmark: stimulus-cycles/s of the interpreter on the SoC-scale synthetic
+design (2^21 clustered random ANDs + reset gates, depth 80, 200k DFFs, 16
+single-port 1024x32 SRAMs, 128 PIs, X-propagation on, all DFF/SRAM state X at
+start, 16 reset cycles then p_toggle = 0.25 stimulus).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+                  [--mode plain|batched] [--lanes L] [--window C]
+
+One step = one launch window of C cycles over all stimulus streams.  `value`
+is device-timed throughput with inputs resident in HBM; `e2e` is the same
+through the C ABI with host buffers copied in and out inside the timed region.
+--impl reference runs the reference's CPU interpreter path (this repository's
+C restatement of it, oracle/) on the host cores.  Multi-GPU: independent
+replicas (one design + its own stimulus streams per rank), weak scaling.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(HERE, "tests"))
+
+LEVEL_SPLIT = tuple(range(5, 80, 5))
+TARGET_CONE = 6000
+RESET_CYCLES = 16
+P_TOGGLE = 0.25
+METRIC = "stimulus-cycles/s bit-exact: batched+learned vs plain kernel vs CPU, 1 B200"
+
+
+def peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu=0):
+        self.gpu = gpu
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._loop, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def build_design(seed=2, clusters=512, n_dff=200_000):
+    from jacquard_b200 import frontend
+    d = frontend.Design(frontend.soc_params(seed=seed, n_clusters=clusters, n_dff=n_dff,
+                                            n_sram=16 if clusters >= 16 else 2))
+    return d
+
+
+def build_script(d, num_blocks, xprop=True):
+    return d.build_script(num_blocks=num_blocks, level_split=LEVEL_SPLIT, xprop=xprop,
+                          target_cone=TARGET_CONE)
+
+
+def algorithmic_bytes_per_cycle(s, lanes=1, arrivals=False):
+    """Bytes one simulated cycle must move (per the boomerang format): script
+    words (counted once per launch pass over `lanes` lane groups), non-empty
+    global-read words, IO read-old + write, SRAM read/read/write, each with
+    its X-mask copy on X-capable partitions; state terms scale with lanes."""
+    bd = s.blocks_data
+    script_words = int(s.blocks_start[-1])
+    gr = io = sr = 0
+    for b in range(s.num_blocks * s.num_major_stages):
+        off = int(s.blocks_start[b])
+        while True:
+            ns = int(bd[off])
+            if ns == 0:
+                break
+            nio, R, nsr, isx = int(bd[off + 2]), int(bd[off + 6]), int(bd[off + 4]), int(bd[off + 8])
+            m = bd[off + 256: off + 256 + 512 * R].reshape(-1, 2)[:, 1]
+            k = 1 + (1 if isx else 0)
+            gr += int(np.count_nonzero(m)) * k
+            io += 2 * nio * k + (nio if arrivals else 0)
+            sr += 3 * nsr * k
+            last = int(bd[off + 1])
+            off += 256 + 512 * R + 5120 * (ns + 2)
+            if last:
+                break
+    return 4 * script_words, 4 * (gr + io + sr) * lanes
+
+
+def stimulus_window(s, d, first_cycle, cycles, seed):
+    """Value+X snapshots for cycles [first_cycle, first_cycle+cycles]: inputs
+    per snapshot, reset held for the first RESET_CYCLES, X template; snapshot
+    0 of the run has every DFF/SRAM word X."""
+    from jacquard_b200 import state
+    rng = np.random.default_rng(seed)
+    vals = state.stimulus_inputs(s, d, first_cycle + cycles, seed, P_TOGGLE, RESET_CYCLES)
+    v = state.pack_inputs(s, vals[first_cycle:first_cycle + cycles + 1])
+    return np.ascontiguousarray(state.expand_states_for_xprop(v, s))
+
+
+def run_mine_plain(args, rank, world):
+    import torch
+    from jacquard_b200 import sim
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
+    nb = sim.max_blocks(dev.index)
+    nb = min(nb, 148 * 3)
+    s = build_script(d, nb)
+    W = args.window
+    eff = 2 * s.reg_io_state_size
+    host = stimulus_window(s, d, 0, W, seed=100 + rank)
+    host_pin = torch.from_numpy(host.view(np.int32).reshape(-1)).pin_memory()
+    out_pin = torch.empty_like(host_pin).pin_memory()
+    ds = sim.DeviceScript(s, dev)
+    st = torch.empty(host_pin.numel(), dtype=torch.int32, device=dev)
+    n_sram = max(1, s.sram_storage_size)
+    sram = torch.zeros(n_sram, dtype=torch.int32, device=dev)
+    sram_x = torch.full((n_sram,), -1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        sim.simulate(ds, st, W, eff, sram, sram_x, stream=stream)
+
+    # warmup (device-resident inputs)
+    st.copy_(host_pin, non_blocking=True)
+    for _ in range(args.warmup):
+        st.copy_(host_pin, non_blocking=True)
+        step()
+    torch.cuda.synchronize()
+    assert sim.status(stream) == 0
+    # timed: device-resident (value).  Each window rewrites the whole snapshot
+    # buffer (W*eff*4 bytes > L2), so no extra flush is needed.
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as ck:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+    dev_ms = t0.elapsed_time(t1)
+    assert sim.status(stream) == 0
+    # timed e2e: pinned host -> device, kernel, device -> host
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st.copy_(host_pin, non_blocking=True)
+        step()
+        out_pin.copy_(st, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    script_b, state_b = algorithmic_bytes_per_cycle(s)
+    return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=1, clocks=ck.summary(),
+                bytes_per_cycle=script_b + state_b, kernel_ms=dev_ms / args.steps,
+                h2d=host_pin.numel() * 4, d2h=out_pin.numel() * 4, launches_per_step=1,
+                design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
+                            script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
+                            major_stages=s.num_major_stages, blocks=nb),
+                script=s, d=d)
+
+
+def cpu_baseline(s, d, cycles=8, threads=1):
+    import oracle_lib
+    host = stimulus_window(s, d, 0, cycles, seed=100)
+    st = host.reshape(-1).copy()
+    n_sram = max(1, s.sram_storage_size)
+    sram = np.zeros(n_sram, np.uint32)
+    sram_x = np.full(n_sram, 0xFFFFFFFF, np.uint32)
+    t = time.perf_counter()
+    oracle_lib.simulate(s, st, cycles, 2 * s.reg_io_state_size, sram=sram, sram_x=sram_x,
+                        threads=threads)
+    dt = time.perf_counter() - t
+    return cycles / dt, dt
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--window", type=int, default=64)
+    ap.add_argument("--cpu-cycles", type=int, default=48)
+    ap.add_argument("--clusters", type=int, default=512,
+                    help="design size in 4096-gate clusters (512 = the 2M-gate workload)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    from jacquard_b200 import build
+    if rank == 0:
+        build.build_all()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        d = build_design()
+        s = build_script(d, 148)
+        threads = os.cpu_count() or 1
+        for _ in range(args.warmup):
+            cpu_baseline(s, d, cycles=1, threads=threads)
+        vals = []
+        for _ in range(args.steps):
+            v, _ = cpu_baseline(s, d, cycles=args.cpu_cycles, threads=threads)
+            vals.append(v)
+        v = float(np.mean(vals))
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "stimulus-cycles/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * args.cpu_cycles / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                "config": {"workload": "soc-2M: 2^21 clustered ANDs + reset gates, depth 80, 200k DFF, 16 SRAM 1024x32, X-prop",
+                           "sample": f"{args.cpu_cycles} cycles per step, 1 stimulus stream"},
+                "cpu_baseline": {"value": v, "unit": "stimulus-cycles/s", "cores": threads,
+                                 "kind": "port",
+                                 "sample": f"{args.cpu_cycles} cycles x 1 stream of the same workload"},
+                "e2e": {"value": v, "unit": "stimulus-cycles/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    r = run_mine_plain(args, rank, world)
+    total_cycles = r["cycles_per_step"] * r["streams"] * args.steps
+    mine_val = total_cycles / (r["dev_ms"] / 1e3)
+    e2e_val = total_cycles / (r["e2e_ms"] / 1e3)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([r["dev_ms"], r["e2e_ms"]], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, e2e_ms = t.tolist()
+        mine_val = world * total_cycles / (dev_ms / 1e3)
+        e2e_val = world * total_cycles / (e2e_ms / 1e3)
+        dist.barrier()
+    if rank == 0:
+        peak, peak_kind = peaks()
+        achieved = r["bytes_per_cycle"] * r["cycles_per_step"] / (r["kernel_ms"] / 1e3) / 1e9
+        if args.no_cpu:
+            cpu_v, cpu_dt = None, 0.0
+        else:
+            cpu_v, cpu_dt = cpu_baseline(r["script"], r["d"], cycles=args.cpu_cycles, threads=1)
+        line = {"metric": METRIC, "value": mine_val, "unit": "stimulus-cycles/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": r["dev_ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                "config": {"workload": "soc-2M: 2^21 clustered ANDs + reset gates, depth 80, 200k DFF, 16 SRAM 1024x32, X-prop",
+                           "mode": args.mode, "streams": r["streams"],
+                           "cycles_per_step": r["cycles_per_step"], "l2": "inputs larger than L2 (snapshot window + script)",
+                           **r["design"]},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
+                "cpu_baseline": {"value": cpu_v, "unit": "stimulus-cycles/s", "cores": 1,
+                                 "kind": "port",
+                                 "sample": f"{args.cpu_cycles} cycles x 1 stream, {cpu_dt:.1f} s"},
+                "e2e": {"value": e2e_val, "unit": "stimulus-cycles/s",
+                        "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+                "gpu_launches": r["launches_per_step"] * args.steps,
+                "clocks": r["clocks"]}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

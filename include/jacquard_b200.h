@@ -107,6 +107,43 @@ int jq_sim_status(void *stream);
 /* Largest grid the plain interpreter can keep co-resident on `device`. */
 int jq_max_blocks(int device, size_t *max_blocks);
 
+/* ------------------------------------------------------------------------ */
+/* Bit-lane batched interpreter: 32*lanes independent stimulus streams run the
+ * same script in one persistent launch.  State is signal-major: snapshot word
+ * [signal * lanes + l] holds one signal (a bit position of the reference
+ * layout, word*32+bit, X plane at metadata word 9 * 32) for streams
+ * 32l..32l+31.  Two snapshot buffers ping-pong: cycle c reads state_a when c
+ * is even (state_b when odd) and writes the other; after num_cycles cycles the
+ * final state is in state_a if num_cycles is even, else state_b.  Both buffers
+ * must start with snapshot 0 (values, X template).  No timing checks. */
+typedef struct {
+  size_t num_blocks, num_major_stages;
+  const size_t *blocks_start;  /* device */
+  const uint32_t *blocks_data; /* device, 16-byte aligned */
+  uint32_t lanes;              /* lane words (32 streams each) */
+  uint32_t *sram_data, *sram_xmask; /* device: [stream][sram_words_per_stream] */
+  size_t sram_words_per_stream;
+  size_t num_cycles;
+  size_t signals_per_snapshot; /* effective state words * 32 */
+  uint32_t *state_a, *state_b;
+  const uint32_t *stimulus;    /* [num_cycles+1][input_signals][lanes] or NULL */
+  size_t input_signals;        /* signals of the input region (words * 32) */
+  const uint32_t *po_signals;  /* signals recorded each cycle */
+  uint32_t n_po;
+  uint32_t *wave;              /* [num_cycles][n_po][lanes] */
+  uint32_t *record;            /* optional [num_cycles+1][signals][lanes] */
+  uint32_t wo_slots;           /* >= the script's largest num_ios (<= 256) */
+  size_t grid;                 /* CTAs; 0 = all that fit */
+  uint64_t barrier_timeout_cycles;
+  void *stream;
+} jq_batch_args;
+
+int jq_simulate_batched(const jq_batch_args *a);
+/* Synchronizes `stream`; JQ_OK or the kernel's recorded error. */
+int jq_batched_status(void *stream);
+int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks);
+int jq_batched_smem_bytes(uint32_t wo_slots);
+
 /* Human-readable text for a status code. */
 const char *jq_strerror(int code);
 

@@ -192,6 +192,18 @@ int64_t jqf_script_array(void *sp, int which, void *dst, size_t cap) {
             tmp.push_back((uint32_t)ms); tmp.push_back((uint32_t)b); tmp.push_back(p);
           }
       break;
+    case 10:
+      // per partition (major stage order): major stage, #stages, cone ANDs,
+      // targets, endpoints
+      for (size_t ms = 0; ms < sc->parts.size(); ++ms)
+        for (const Partition &p : sc->parts[ms]) {
+          tmp.push_back((uint32_t)ms);
+          tmp.push_back((uint32_t)p.stages.size());
+          tmp.push_back(p.cone_ands);
+          tmp.push_back(p.targets);
+          tmp.push_back((uint32_t)p.endpoints.size());
+        }
+      break;
     default: return -1;
   }
   if (!src) { src = tmp.data(); bytes = tmp.size() * 4; }

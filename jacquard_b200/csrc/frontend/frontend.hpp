@@ -65,6 +65,8 @@ struct BoomStage {
 struct Partition {
   std::vector<uint32_t> endpoints;  // staged endpoint ids
   std::vector<BoomStage> stages;
+  uint32_t cone_ands = 0;  // AND gates in the partition's cone
+  uint32_t targets = 0;    // distinct endpoint input pins
 };
 struct PackOptions {
   int max_stages = 64;

@@ -129,6 +129,9 @@ bool build_partition(const AIG &g, const StagedAIG &st,
   }
   const int n = (int)C.pin.size();
   for (uint32_t t : targets) C.tgt[loc.at(t)] = 1;
+  out.targets = (uint32_t)targets.size();
+  out.cone_ands = 0;
+  for (int i = 0; i < n; ++i) out.cone_ands += !C.leaf[i];
   {
     std::vector<uint32_t> deg(n + 1, 0);
     for (int i = 0; i < n; ++i)

@@ -215,6 +215,8 @@ class Script:
             self.dff_data_pos = arr(7, np.uint32)
             self.input_layout = arr(8, np.uint32)
             self.stage_block_part = arr(9, np.uint32).reshape(-1, 3)
+            # (major stage, #boomerang stages, cone ANDs, targets, endpoints)
+            self.partition_stats = arr(10, np.uint32).reshape(-1, 5)
         finally:
             lib.jqf_free_script(h)
         self.timing_arrivals_enabled = False

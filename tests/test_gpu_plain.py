@@ -89,7 +89,7 @@ def test_plain_timing_events_and_arrivals_match_oracle():
     s = cases.script("sram", 16, (8,), timing_seed=9)
     s.enable_timing_arrivals()
     states = cases.stimulus("sram", s, 24)
-    cons = cases.constraint_buffer("sram", s, clock_ps=300, setup=30, hold=60)
+    cons = cases.constraint_buffer("sram", s, clock_ps=120, setup=30, hold=150)
     want, _, _, (wev, wcnt) = run_oracle(s, states, 24, constraints=cons, cap=1 << 16,
                                          arrival_off=s.arrival_state_offset)
     got, _, _, (gev, gcnt, gov) = run_gpu(s, states, 24, constraints=cons, cap=1 << 16,
