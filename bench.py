@@ -208,6 +208,85 @@ def run_mine_plain(args, rank, world):
                 script=s, d=d)
 
 
+def batched_stimulus(s, d, streams, cycles, seed0, first=0):
+    """(cycles+1, input_signals, lanes) input lane words: stream k uses seed
+    seed0 + k (reset for the first RESET_CYCLES, then p_toggle inputs)."""
+    from jacquard_b200 import batched, state
+    words = batched.input_words(s)
+    per = np.zeros((streams, cycles + 1, words), np.uint32)
+    for k in range(streams):
+        vals = state.stimulus_inputs(s, d, first + cycles, seed0 + k, P_TOGGLE, RESET_CYCLES)
+        per[k] = state.pack_inputs(s, vals[first:first + cycles + 1])[:, :words]
+    return batched.to_batched(per)
+
+
+def run_mine_batched(args, rank, world):
+    import torch
+    from jacquard_b200 import batched, state
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
+    s = build_script(d, args.blocks)
+    lanes = args.lanes
+    streams = 32 * lanes
+    W = args.window
+    assert W % 2 == 0, "even windows keep the final state in buffer A"
+    po_sig = state.po_positions(s, d)
+    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
+    # snapshot 0: inputs of cycle 0, every DFF/SRAM word X
+    stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
+    snap0 = np.zeros((B.sig, lanes), np.uint32)
+    xt = state.xmask_template(s)
+    rio = s.reg_io_state_size
+    xt_b = batched.to_batched(np.repeat(xt[None, :], streams, axis=0))
+    snap0[rio * 32:2 * rio * 32] = xt_b
+    snap0[:B.in_sigs] = stim[0]
+    B.load_state(snap0)
+    B.reset_sram(x=True)
+    stim_pin = torch.from_numpy(np.ascontiguousarray(stim).reshape(-1).view(np.int32)).pin_memory()
+    stim_dev = torch.empty(stim_pin.numel(), dtype=torch.int32, device=dev)
+    stim_dev.copy_(stim_pin)
+    wave = torch.empty(W * len(po_sig) * lanes, dtype=torch.int32, device=dev)
+    wave_pin = torch.empty(wave.numel(), dtype=torch.int32).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        B.run(stim_dev, W, wave=wave, stream=stream)
+    torch.cuda.synchronize()
+    assert B.status(stream) == 0
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as ck:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(args.steps):
+            B.run(stim_dev, W, wave=wave, stream=stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    dev_ms = t0.elapsed_time(t1)
+    assert B.status(stream) == 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        stim_dev.copy_(stim_pin, non_blocking=True)
+        B.run(stim_dev, W, wave=wave, stream=stream)
+        wave_pin.copy_(wave, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    assert B.status(stream) == 0
+    script_b, state_b = algorithmic_bytes_per_cycle(s)
+    return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams,
+                clocks=ck.summary(), bytes_per_cycle=script_b + state_b * streams,
+                kernel_ms=dev_ms / args.steps, h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4,
+                launches_per_step=1,
+                design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
+                            script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
+                            major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes),
+                script=s, d=d)
+
+
 def cpu_baseline(s, d, cycles=8, threads=1):
     import oracle_lib
     host = stimulus_window(s, d, 0, cycles, seed=100)
@@ -228,8 +307,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--mode", default="batched", choices=["plain", "batched"])
     ap.add_argument("--window", type=int, default=64)
+    ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
+    ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
     ap.add_argument("--cpu-cycles", type=int, default=48)
     ap.add_argument("--clusters", type=int, default=512,
                     help="design size in 4096-gate clusters (512 = the 2M-gate workload)")
@@ -272,7 +353,7 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    r = run_mine_plain(args, rank, world)
+    r = run_mine_batched(args, rank, world) if args.mode == "batched" else run_mine_plain(args, rank, world)
     total_cycles = r["cycles_per_step"] * r["streams"] * args.steps
     mine_val = total_cycles / (r["dev_ms"] / 1e3)
     e2e_val = total_cycles / (r["e2e_ms"] / 1e3)

@@ -133,32 +133,70 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
       tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
     }
 
-    // ---- global read: thread t (< 256) gathers its (idx, mask) pairs
+    // ---- global read, in two phases so that the loads overlap:
+    // (a) thread t < 256 enumerates its (idx, mask) bits and stores, at the
+    //     destination position, the source signal (bit 31 = current-cycle
+    //     staged IO) or NONE for the unfilled tail; positions follow the
+    //     kernel's append order (first appended bit ends up most significant);
+    // (b) all threads load their 16 positions with independent loads.
     if (t < 256) {
+      // all (idx, mask) pairs of this thread in flight at once (R <= 16 in
+      // registers; longer lists are read a second time from global)
+      uint2 pr[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) pr[r] = (uint32_t)r < R ? ldg2(gr + 512 * r + 2 * t) : make_uint2(0, 0);
       uint32_t total = 0;
-      for (uint32_t r = 0; r < R; ++r) total += __popc(__ldg(gr + 512 * r + 2 * t + 1));
+#pragma unroll
+      for (int r = 0; r < 16; ++r) total += __popc(pr[r].y);
+      for (uint32_t r = 16; r < R; ++r) total += __popc(__ldg(gr + 512 * r + 2 * t + 1));
       uint32_t i = 0;
-      for (uint32_t r = 0; r < R; ++r) {
-        const uint2 im = ldg2(gr + 512 * r + 2 * t);
-        uint32_t m = im.y;
-        const uint32_t *base = (im.x >> 31) ? out : in;
-        const size_t w = im.x & 0x7fffffffu;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        uint32_t m = pr[r].y;
+        const uint32_t stg = pr[r].x & 0x80000000u;
+        const uint32_t w = pr[r].x & 0x7fffffffu;
         while (m) {
           const uint32_t k = __ffs(m) - 1;
           m &= m - 1;
-          const size_t sg = (w * 32 + k) * L + lane;
-          const uint32_t pos = 32 * t + (total - 1 - i);
-          S[pos] = ldcg(base + sg);
-          if (is_x) SX[pos] = ldcg(base + (size_t)xsig * L + sg);
+          S[32 * t + (total - 1 - i)] = stg | (w * 32 + k);
           ++i;
         }
       }
-      for (uint32_t k = total; k < 32; ++k) {
-        S[32 * t + k] = 0;
-        SX[32 * t + k] = 0;
+      for (uint32_t r = 16; r < R; ++r) {
+        const uint2 im = ldg2(gr + 512 * r + 2 * t);
+        uint32_t m = im.y;
+        const uint32_t stg = im.x & 0x80000000u;
+        const uint32_t w = im.x & 0x7fffffffu;
+        while (m) {
+          const uint32_t k = __ffs(m) - 1;
+          m &= m - 1;
+          S[32 * t + (total - 1 - i)] = stg | (w * 32 + k);
+          ++i;
+        }
       }
-      if (!is_x)
-        for (uint32_t k = 0; k < total; ++k) SX[32 * t + k] = 0;
+      for (uint32_t k = total; k < 32; ++k) S[32 * t + k] = 0xffffffffu;
+    }
+    __syncthreads();
+    {
+      uint32_t e[16], v[16], vx[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) e[k] = S[t + BT * k];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        v[k] = 0;
+        vx[k] = 0;
+        if (e[k] != 0xffffffffu) {
+          const uint32_t *base = (e[k] >> 31) ? out : in;
+          const size_t sg = (size_t)(e[k] & 0x7fffffffu) * L + lane;
+          v[k] = ldcg(base + sg);
+          if (is_x) vx[k] = ldcg(base + (size_t)xsig * L + sg);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        S[t + BT * k] = v[k];
+        SX[t + BT * k] = vx[k];
+      }
     }
 
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
@@ -364,21 +402,38 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
           WOX[dst] = SX[num_srams * 4 * 32 + q];
         }
       } else {
-        // ---------------- clock-enable permutation and commit
-        for (uint32_t q = t; q < num_ios * 32; q += BT) {
-          const uint32_t src = perm_at(C, q);
-          const uint32_t fw = (q >> 5) * 4;
-          const uint32_t inv = bitmask(F[fw], q), set0 = bitmask(F[fw + 1], q),
-                         dinv = bitmask(F[fw + 2], q);
-          const uint32_t cp = (WO[src] & ~set0) ^ inv;
-          const uint32_t wv = WO[q] ^ dinv;
-          const size_t sg = ((size_t)io_off * 32 + q) * L + lane;
-          const uint32_t old = ldcg(in + sg);
-          out[sg] = (old & ~cp) | (wv & cp);
-          if (is_x) {
-            const uint32_t cpx = WOX[src] & ~set0;
-            const uint32_t oldx = ldcg(in + (size_t)xsig * L + sg);
-            out[(size_t)xsig * L + sg] = (oldx & ~cp & ~cpx) | (WOX[q] & cp & ~cpx) | cpx;
+        // ---------------- clock-enable permutation and commit (4 words per
+        // thread in flight)
+        const uint32_t nq = num_ios * 32;
+        for (uint32_t q0 = t; q0 < nq; q0 += 4 * BT) {
+          uint32_t cp[4], cpx[4], wv[4], wx[4], old[4], oldx[4];
+          size_t sg[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t q = q0 + u * BT;
+            if (q < nq) {
+              const uint32_t src = perm_at(C, q);
+              const uint32_t fw = (q >> 5) * 4;
+              const uint32_t inv = bitmask(F[fw], q), set0 = bitmask(F[fw + 1], q),
+                             dinv = bitmask(F[fw + 2], q);
+              cp[u] = (WO[src] & ~set0) ^ inv;
+              cpx[u] = is_x ? (WOX[src] & ~set0) : 0u;
+              wv[u] = WO[q] ^ dinv;
+              wx[u] = WOX[q];
+              sg[u] = ((size_t)io_off * 32 + q) * L + lane;
+              old[u] = ldcg(in + sg[u]);
+              oldx[u] = is_x ? ldcg(in + (size_t)xsig * L + sg[u]) : 0u;
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t q = q0 + u * BT;
+            if (q < nq) {
+              out[sg[u]] = (old[u] & ~cp[u]) | (wv[u] & cp[u]);
+              if (is_x)
+                out[(size_t)xsig * L + sg[u]] =
+                    (oldx[u] & ~cp[u] & ~cpx[u]) | (wx[u] & cp[u] & ~cpx[u]) | cpx[u];
+            }
           }
         }
       }
