@@ -209,7 +209,7 @@ def run_mine_plain(args, rank, world):
 
 
 def batched_stimulus(s, d, streams, cycles, seed0, first=0):
-    """(cycles+1, input_signals, lanes) input lane words: stream k uses seed
+    """(cycles+1, lanes, input_signals) input lane words: stream k uses seed
     seed0 + k (reset for the first RESET_CYCLES, then p_toggle inputs)."""
     from jacquard_b200 import batched, state
     words = batched.input_words(s)
@@ -235,12 +235,12 @@ def run_mine_batched(args, rank, world):
     B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
     # snapshot 0: inputs of cycle 0, every DFF/SRAM word X
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
-    snap0 = np.zeros((B.sig, lanes), np.uint32)
+    snap0 = np.zeros((lanes, B.sig), np.uint32)
     xt = state.xmask_template(s)
     rio = s.reg_io_state_size
     xt_b = batched.to_batched(np.repeat(xt[None, :], streams, axis=0))
-    snap0[rio * 32:2 * rio * 32] = xt_b
-    snap0[:B.in_sigs] = stim[0]
+    snap0[:, rio * 32:2 * rio * 32] = xt_b
+    snap0[:, :B.in_sigs] = stim[0]
     B.load_state(snap0)
     B.reset_sram(x=True)
     stim_pin = torch.from_numpy(np.ascontiguousarray(stim).reshape(-1).view(np.int32)).pin_memory()

@@ -109,10 +109,10 @@ int jq_max_blocks(int device, size_t *max_blocks);
 
 /* ------------------------------------------------------------------------ */
 /* Bit-lane batched interpreter: 32*lanes independent stimulus streams run the
- * same script in one persistent launch.  State is signal-major: snapshot word
- * [signal * lanes + l] holds one signal (a bit position of the reference
- * layout, word*32+bit, X plane at metadata word 9 * 32) for streams
- * 32l..32l+31.  Two snapshot buffers ping-pong: cycle c reads state_a when c
+ * same script in one persistent launch.  State is lane-major: snapshot word
+ * [l * signals_per_snapshot + signal] holds one signal (a bit position of the
+ * reference layout, word*32+bit, X plane at metadata word 9 * 32) for
+ * streams 32l..32l+31.  Two snapshot buffers ping-pong: cycle c reads state_a when c
  * is even (state_b when odd) and writes the other; after num_cycles cycles the
  * final state is in state_a if num_cycles is even, else state_b.  Both buffers
  * must start with snapshot 0 (values, X template).  No timing checks. */
@@ -126,13 +126,28 @@ typedef struct {
   size_t num_cycles;
   size_t signals_per_snapshot; /* effective state words * 32 */
   uint32_t *state_a, *state_b;
-  const uint32_t *stimulus;    /* [num_cycles+1][input_signals][lanes] or NULL */
-  size_t input_signals;        /* signals of the input region (words * 32) */
+  const uint32_t *stimulus;    /* [num_cycles+1][lanes][input_signals] or NULL */
+  size_t input_signals;        /* stimulus signals per lane and cycle */
+  const uint32_t *input_regions; /* device: (state signal, stimulus signal, count)
+                                    triples, or NULL for one region at 0 (used
+                                    when several designs share one state) */
+  uint32_t n_input_regions;
   const uint32_t *po_signals;  /* signals recorded each cycle */
   uint32_t n_po;
   uint32_t *wave;              /* [num_cycles][n_po][lanes] */
-  uint32_t *record;            /* optional [num_cycles+1][signals][lanes] */
+  uint32_t *record;            /* optional [num_cycles+1][lanes][signals] */
   uint32_t wo_slots;           /* >= the script's largest num_ios (<= 256) */
+  const uint32_t *block_list;  /* device: blocks with work, per major stage
+                                  (any order; heaviest first is best), or NULL
+                                  for all blocks */
+  const uint32_t *block_list_start; /* device: num_major_stages+1 offsets */
+  unsigned long long *part_cycles; /* optional device output: SM clocks spent
+                                      per partition, summed over lanes and
+                                      cycles (partition order of the script:
+                                      major stage, block, position in block) */
+  const uint32_t *part_base;   /* device: index of the first partition of each
+                                  (major stage, block); required with
+                                  part_cycles */
   size_t grid;                 /* CTAs; 0 = all that fit */
   uint64_t barrier_timeout_cycles;
   void *stream;
@@ -143,6 +158,47 @@ int jq_simulate_batched(const jq_batch_args *a);
 int jq_batched_status(void *stream);
 int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks);
 int jq_batched_smem_bytes(uint32_t wo_slots);
+
+/* ------------------------------------------------------------------------ */
+/* Partition cost model (no counterpart in the reference): an MLP
+ * JQ_MLP_FEATURES -> 128 -> 128 -> 1 (ReLU) predicting log kernel time of a
+ * partition from its features.  BF16 weights/activations, FP32 accumulation.
+ * theta is the fp32 master parameter vector (JQ_MLP_PARAMS floats:
+ * W1[128][24] b1[128] W2[128][128] b2[128] W3[128] b3), theta16 its bf16 copy
+ * (uint16 storage).  X holds normalised features as bf16 [n][24]. */
+#define JQ_MLP_FEATURES 24
+#define JQ_MLP_HIDDEN 128
+#define JQ_MLP_PARAMS (128 * 24 + 128 + 128 * 128 + 128 + 128 + 1)
+
+/* theta16 <- bf16(theta). */
+int jq_mlp_sync_bf16(const float *theta, uint16_t *theta16, void *stream);
+/* y[i] = model(X[i]) for n rows. */
+int jq_mlp_forward(const float *theta, const uint16_t *theta16, const uint16_t *X, size_t n,
+                   float *y, void *stream);
+
+typedef struct {
+  float *theta;          /* device fp32 master parameters (updated when apply) */
+  uint16_t *theta16;     /* device bf16 copy (updated when apply) */
+  float *adam_m, *adam_v; /* device Adam moments (JQ_MLP_PARAMS each) */
+  const uint16_t *X;     /* device bf16 features [rows][24] */
+  const float *T;        /* device targets [rows] */
+  const uint32_t *batch_index; /* device row indices of this mini-batch */
+  uint32_t batch;
+  uint32_t step;         /* Adam step, 1-based */
+  float lr;
+  int32_t apply;         /* 0: gradient only (grad_out), 1: Adam update */
+  float *grad_out;       /* optional device [JQ_MLP_PARAMS] summed gradient */
+  float *loss_out;       /* optional device scalar: mean squared error */
+  float *scratch;        /* device workspace, jq_mlp_scratch_floats(scratch_ctas) */
+  uint32_t scratch_ctas; /* CTAs that split the batch (one gradient row each) */
+  void *stream;
+} jq_mlp_step_args;
+
+/* Floats of workspace jq_mlp_train_step needs for `ctas` CTAs. */
+size_t jq_mlp_scratch_floats(uint32_t ctas);
+/* One mini-batch: forward, backward of the mean squared error, gradient
+ * reduction and (apply=1) an Adam step (beta1 0.9, beta2 0.999, eps 1e-8). */
+int jq_mlp_train_step(const jq_mlp_step_args *a);
 
 /* Human-readable text for a status code. */
 const char *jq_strerror(int code);

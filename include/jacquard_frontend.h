@@ -57,7 +57,16 @@ typedef struct {
   uint32_t target_endpoint_bits;
   int32_t num_threads;         /* 0 = all host threads */
   int32_t merge_passes;
+  /* Optional learned partition cost model (JQF_COST_MODEL_FLOATS floats:
+   * W1[128][24] b1[128] W2[128][128] b2[128] W3[128] b3, then feature mean[24]
+   * and 1/std[24]).  When set, partition merges are accepted when the
+   * predicted kernel time of the merged partition is below the sum of the
+   * two; otherwise the stage-count rule is used. */
+  const float *cost_model;
 } jqf_build_params;
+
+#define JQF_FEATURES 24
+#define JQF_COST_MODEL_FLOATS (128 * 24 + 128 + 128 * 128 + 128 + 128 + 1 + 24 + 24)
 
 typedef struct {
   uint64_t num_blocks, num_major_stages, blocks_data_len;
@@ -70,6 +79,12 @@ void *jqf_build_script(void *design, const jqf_build_params *bp, char *err, size
 void jqf_free_script(void *script);
 int jqf_script_info(void *script, jqf_script_info_t *out);
 int64_t jqf_script_array(void *script, int which, void *dst, size_t cap);
+
+/* Features of every partition of a built script, in script order (major
+ * stage, block, position): num_partitions x JQF_FEATURES floats. */
+int jqf_script_features(void *design, void *script, float *out);
+/* Host inference of a cost model on `n` feature rows (log kernel cycles). */
+int jqf_cost_model_predict(const float *model, const float *features, size_t n, float *out);
 
 /* Host-side script validator (same walk as the kernel). 0 = valid. */
 int jqf_validate(const uint64_t *blocks_start, size_t num_blocks, size_t num_major_stages,

@@ -22,8 +22,11 @@ class BatchArgs(ctypes.Structure):
                 ("sram_data", vp), ("sram_xmask", vp), ("sram_words_per_stream", ctypes.c_size_t),
                 ("num_cycles", ctypes.c_size_t), ("signals_per_snapshot", ctypes.c_size_t),
                 ("state_a", vp), ("state_b", vp), ("stimulus", vp), ("input_signals", ctypes.c_size_t),
+                ("input_regions", vp), ("n_input_regions", ctypes.c_uint32),
                 ("po_signals", vp), ("n_po", ctypes.c_uint32), ("wave", vp), ("record", vp),
-                ("wo_slots", ctypes.c_uint32), ("grid", ctypes.c_size_t),
+                ("wo_slots", ctypes.c_uint32), ("block_list", vp), ("block_list_start", vp),
+                ("part_cycles", vp), ("part_base", vp),
+                ("grid", ctypes.c_size_t),
                 ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp)]
 
 
@@ -41,8 +44,9 @@ def lib():
 
 
 def to_batched(per_stream):
-    """(streams, ..., words) u32 per-stream layout -> (..., words*32, lanes)
-    signal-major lane words (streams must be a multiple of 32)."""
+    """(streams, ..., words) u32 per-stream layout -> (..., lanes, words*32)
+    lane-major lane words: word [l, signal] holds `signal` of streams
+    32l..32l+31 (bit i = stream 32l+i).  streams must be a multiple of 32."""
     a = np.asarray(per_stream, dtype=np.uint32)
     S = a.shape[0]
     assert S % 32 == 0
@@ -50,13 +54,13 @@ def to_batched(per_stream):
     bits = bits.reshape(a.shape[:-1] + (a.shape[-1] * 32,))       # (S, ..., sig)
     bits = np.moveaxis(bits, 0, -1)                                # (..., sig, S)
     packed = np.packbits(bits, axis=-1, bitorder="little")        # (..., sig, S/8)
-    return np.ascontiguousarray(packed).view(np.uint32)           # (..., sig, lanes)
+    words = np.ascontiguousarray(packed).view(np.uint32)          # (..., sig, lanes)
+    return np.ascontiguousarray(np.swapaxes(words, -1, -2))      # (..., lanes, sig)
 
 
 def from_batched(batched, words):
-    """Inverse of to_batched: (..., sig, lanes) -> (streams, ..., words)."""
-    b = np.ascontiguousarray(batched, dtype=np.uint32)
-    lanes = b.shape[-1]
+    """Inverse of to_batched: (..., lanes, sig) -> (streams, ..., words)."""
+    b = np.ascontiguousarray(np.swapaxes(np.asarray(batched, dtype=np.uint32), -1, -2))
     bits = np.unpackbits(b.view(np.uint8), axis=-1, bitorder="little")  # (..., sig, S)
     bits = np.moveaxis(bits, -1, 0).astype(np.uint32)              # (S, ..., sig)
     bits = bits.reshape(bits.shape[:-1] + (words, 32))
@@ -72,20 +76,42 @@ def input_words(script):
     return w
 
 
+def block_work(script):
+    """Per (major stage, block): (boomerang stages + 2 per partition, max num_ios)."""
+    bd = script.blocks_data
+    nb, nms = script.num_blocks, script.num_major_stages
+    work = np.zeros((nms, nb), np.int64)
+    mio = 0
+    for ms in range(nms):
+        for b in range(nb):
+            off = int(script.blocks_start[ms * nb + b])
+            while True:
+                ns = int(bd[off])
+                if ns == 0:
+                    break
+                mio = max(mio, int(bd[off + 2]))
+                work[ms, b] += ns + 2
+                R, last = int(bd[off + 6]), int(bd[off + 1])
+                off += 256 + 512 * R + 5120 * (ns + 2)
+                if last:
+                    break
+    return work, mio
+
+
 def max_num_ios(script):
-    bd, m = script.blocks_data, 0
-    for b in range(script.num_blocks * script.num_major_stages):
-        off = int(script.blocks_start[b])
-        while True:
-            ns = int(bd[off])
-            if ns == 0:
-                break
-            m = max(m, int(bd[off + 2]))
-            R, last = int(bd[off + 6]), int(bd[off + 1])
-            off += 256 + 512 * R + 5120 * (ns + 2)
-            if last:
-                break
-    return m
+    return block_work(script)[1]
+
+
+def block_lists(script):
+    """Non-empty blocks of each major stage, heaviest first, and offsets."""
+    work, _ = block_work(script)
+    lst, start = [], [0]
+    for ms in range(work.shape[0]):
+        nz = np.nonzero(work[ms])[0]
+        nz = nz[np.argsort(-work[ms][nz], kind="stable")]
+        lst.extend(nz.tolist())
+        start.append(len(lst))
+    return np.asarray(lst if lst else [0], np.uint32), np.asarray(start, np.uint32)
 
 
 class BatchedSim:
@@ -96,10 +122,21 @@ class BatchedSim:
         self.lanes = lanes
         self.device = torch.device(device)
         self.ds = sim.DeviceScript(script, self.device)
-        self.eff = script.reg_io_state_size * (2 if script.xprop_enabled else 1)
+        self.eff = getattr(script, "effective_words", None) or \
+            script.reg_io_state_size * (2 if script.xprop_enabled else 1)
         self.sig = self.eff * 32
-        self.in_sigs = input_words(script) * 32
+        regions = getattr(script, "input_regions", None)
+        if regions is None:
+            self.in_sigs = input_words(script) * 32
+            self.regions = None
+        else:
+            r = np.asarray(regions, np.uint32).reshape(-1, 3)
+            self.in_sigs = int(r[:, 2].sum())
+            self.regions = torch.from_numpy(r.reshape(-1).view(np.int32)).to(self.device)
         self.wo_slots = max(1, max_num_ios(script))
+        bl, bls = block_lists(script)
+        self.block_list = torch.from_numpy(bl.view(np.int32)).to(self.device)
+        self.block_list_start = torch.from_numpy(bls.view(np.int32)).to(self.device)
         self.sram_words = max(1, script.sram_storage_size)
         n_streams = 32 * lanes
         self.state_a = torch.zeros(self.sig * lanes, dtype=torch.int32, device=self.device)
@@ -113,7 +150,7 @@ class BatchedSim:
         self.grid = grid
 
     def load_state(self, snap0):
-        """snap0: (sig, lanes) u32 batched snapshot 0 (values + X template)."""
+        """snap0: (lanes, sig) u32 batched snapshot 0 (values + X template)."""
         t = torch.from_numpy(np.ascontiguousarray(snap0, np.uint32).reshape(-1).view(np.int32)).to(self.device)
         self.state_a.copy_(t)
         self.state_b.copy_(t)
@@ -122,8 +159,22 @@ class BatchedSim:
         self.sram.zero_()
         self.sram_x.fill_(-1 if x else 0)
 
-    def run(self, stim, cycles, wave=None, record_buf=None, stream=None):
-        """stim: device tensor [(cycles+1) * in_sigs * lanes] int32 or None."""
+    def part_base(self):
+        """Index of the first partition of each (major stage, block)."""
+        sbp = self.script.stage_block_part
+        nb = self.script.num_blocks
+        base = np.zeros(self.script.num_major_stages * nb, np.uint32)
+        seen = {}
+        for i, (ms, b, _) in enumerate(sbp.tolist()):
+            seen.setdefault(ms * nb + b, i)
+        nxt = len(sbp)
+        for k in range(base.size - 1, -1, -1):
+            nxt = seen.get(k, nxt)
+            base[k] = nxt
+        return base
+
+    def run(self, stim, cycles, wave=None, record_buf=None, stream=None, part_cycles=None):
+        """stim: device tensor [(cycles+1) * lanes * in_sigs] int32 or None."""
         L = lib()
         wave_ptr = wave.data_ptr() if wave is not None else None
         a = BatchArgs(self.ds.num_blocks, self.ds.num_major_stages, self.ds.blocks_start.data_ptr(),
@@ -131,13 +182,23 @@ class BatchedSim:
                       self.sram_x.data_ptr(), self.sram_words, cycles, self.sig,
                       self.state_a.data_ptr(), self.state_b.data_ptr(),
                       stim.data_ptr() if stim is not None else None, self.in_sigs,
+                      self.regions.data_ptr() if self.regions is not None else None,
+                      0 if self.regions is None else self.regions.numel() // 3,
                       self.po.data_ptr(), self.n_po, wave_ptr,
                       record_buf.data_ptr() if record_buf is not None else None,
-                      self.wo_slots, self.grid, 0,
+                      self.wo_slots, self.block_list.data_ptr(), self.block_list_start.data_ptr(),
+                      part_cycles.data_ptr() if part_cycles is not None else None,
+                      self._part_base().data_ptr() if part_cycles is not None else None,
+                      self.grid, 0,
                       stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         rc = L.jq_simulate_batched(ctypes.byref(a))
         if rc:
             raise RuntimeError("jq_simulate_batched: " + sim.lib().jq_strerror(rc).decode())
+
+    def _part_base(self):
+        if getattr(self, "_pb", None) is None:
+            self._pb = torch.from_numpy(self.part_base().view(np.int32)).to(self.device)
+        return self._pb
 
     def status(self, stream=None):
         s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
@@ -145,3 +206,90 @@ class BatchedSim:
 
     def final_state(self, cycles):
         return self.state_a if cycles % 2 == 0 else self.state_b
+
+
+class CombinedScript:
+    """Several designs' scripts relocated into one script and one state so a
+    single persistent launch runs them all (work items of every design share
+    the CTAs; designs with fewer major stages leave empty blocks).
+
+    Relocation only shifts absolute offsets: IO offset (metadata word 3), SRAM
+    offset (word 5) and global-read word indices move by the design's state /
+    SRAM base; the X offset (word 9) stays the design's own value-plane size
+    because each design keeps its [values | X] pair contiguous."""
+
+    def __init__(self, scripts):
+        self.parts = scripts
+        self.xprop_enabled = True
+        nms = max(s.num_major_stages for s in scripts)
+        self.num_major_stages = nms
+        self.num_blocks = sum(s.num_blocks for s in scripts)
+        self.state_base, self.sram_base, self.block_base = [], [], []
+        sb = srb = bb = 0
+        for s in scripts:
+            assert s.xprop_enabled, "designs are combined with X-propagation on"
+            self.state_base.append(sb)
+            self.sram_base.append(srb)
+            self.block_base.append(bb)
+            sb += 2 * s.reg_io_state_size
+            srb += s.sram_storage_size
+            bb += s.num_blocks
+        self.effective_words = sb
+        self.sram_storage_size = srb
+        self.reg_io_state_size = sb // 2  # not used for layout (effective_words is)
+        data, starts, sbp = [], [], []
+        pos = 0
+        dummy = np.zeros(256, np.uint32)
+        dummy[1] = 1
+        pidx = 0
+        for ms in range(nms):
+            for d, s in enumerate(scripts):
+                for b in range(s.num_blocks):
+                    starts.append(pos)
+                    if ms >= s.num_major_stages:
+                        data.append(dummy)
+                        pos += 256
+                        continue
+                    lo = int(s.blocks_start[ms * s.num_blocks + b])
+                    hi = int(s.blocks_start[ms * s.num_blocks + b + 1])
+                    blk = s.blocks_data[lo:hi].copy()
+                    off = 0
+                    while True:
+                        ns = int(blk[off])
+                        if ns == 0:
+                            break
+                        R = int(blk[off + 6])
+                        blk[off + 3] += self.state_base[d]
+                        blk[off + 5] += self.sram_base[d]
+                        g = blk[off + 256: off + 256 + 512 * R].reshape(-1, 2)
+                        nz = g[:, 1] != 0
+                        hi_bit = g[:, 0] & np.uint32(0x80000000)
+                        g[:, 0] = np.where(nz, hi_bit | ((g[:, 0] & np.uint32(0x7FFFFFFF)) +
+                                                         np.uint32(self.state_base[d])), g[:, 0])
+                        sbp.append((ms, self.block_base[d] + b, pidx))
+                        pidx += 1
+                        last = int(blk[off + 1])
+                        off += 256 + 512 * R + 5120 * (ns + 2)
+                        if last:
+                            break
+                    data.append(blk)
+                    pos += blk.size
+        starts.append(pos)
+        data.append(np.zeros(8 * 256, np.uint32))
+        self.blocks_data = np.concatenate(data).astype(np.uint32)
+        self.blocks_start = np.asarray(starts, np.uint64)
+        self.stage_block_part = np.asarray(sbp, np.uint32).reshape(-1, 3)
+        # stimulus: each design's input signals, concatenated per lane
+        regions, src = [], 0
+        for d, s in enumerate(scripts):
+            n = input_words(s) * 32
+            regions.append((self.state_base[d] * 32, src, n))
+            src += n
+        self.input_regions = regions
+
+    def script_words_per_cycle(self):
+        return int(self.blocks_start[-1])
+
+    def signal(self, d, sig):
+        """Combined signal index of design d's signal `sig`."""
+        return self.state_base[d] * 32 + sig

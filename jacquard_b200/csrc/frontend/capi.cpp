@@ -14,6 +14,25 @@ struct Design {
   AIG g;
   GenInfo info;
 };
+CostModel unpack_model(const float *m) {
+  CostModel cm;
+  const int NF = NFEAT, H = 128;
+  cm.w1.assign(m, m + H * NF);
+  m += H * NF;
+  cm.b1.assign(m, m + H);
+  m += H;
+  cm.w2.assign(m, m + H * H);
+  m += H * H;
+  cm.b2.assign(m, m + H);
+  m += H;
+  cm.w3.assign(m, m + H);
+  m += H;
+  cm.b3 = *m++;
+  cm.mean.assign(m, m + NF);
+  m += NF;
+  cm.inv_std.assign(m, m + NF);
+  return cm;
+}
 struct Script {
   FlatScript s;
   std::vector<StagedAIG> stageds;
@@ -119,6 +138,16 @@ void *jqf_build_script(void *dp, const jqf_build_params *bp, char *err, size_t e
     if (bp->target_endpoint_bits) po.target_endpoint_bits = bp->target_endpoint_bits;
     po.num_threads = bp->num_threads;
     po.merge_passes = bp->merge_passes;
+    CostModel cm;
+    std::vector<uint8_t> xp;
+    if (bp->cost_model) {
+      cm = unpack_model(bp->cost_model);
+      po.cost_model = &cm;
+      if (bp->xprop) {
+        xp = d->g.x_capable_pins();
+        po.xpins = &xp;
+      }
+    }
     for (auto &st : sc->stageds) sc->parts.push_back(partition_stage(d->g, st, po));
     FlattenOptions fo;
     fo.num_blocks = bp->num_blocks;
@@ -209,6 +238,23 @@ int64_t jqf_script_array(void *sp, int which, void *dst, size_t cap) {
   if (!src) { src = tmp.data(); bytes = tmp.size() * 4; }
   if (dst && cap >= bytes) std::memcpy(dst, src, bytes);
   return (int64_t)bytes;
+}
+
+int jqf_script_features(void *dp, void *sp, float *out) {
+  auto *d = static_cast<Design *>(dp);
+  auto *sc = static_cast<Script *>(sp);
+  std::vector<uint8_t> xp;
+  if (sc->s.xprop_enabled) xp = d->g.x_capable_pins();
+  for (size_t i = 0; i < sc->s.part_ptrs.size(); ++i)
+    partition_features(d->g, sc->stageds[sc->s.part_major_stage[i]], *sc->s.part_ptrs[i],
+                       sc->s.xprop_enabled ? &xp : nullptr, out + i * NFEAT);
+  return 0;
+}
+
+int jqf_cost_model_predict(const float *model, const float *features, size_t n, float *out) {
+  CostModel cm = unpack_model(model);
+  for (size_t i = 0; i < n; ++i) out[i] = cm.predict(features + i * NFEAT);
+  return 0;
 }
 
 int jqf_validate(const uint64_t *blocks_start, size_t num_blocks, size_t num_major_stages,

@@ -600,6 +600,8 @@ bool flatten_script(const AIG &g, const std::vector<StagedAIG> &stageds,
     for (size_t b = 0; b < nb; ++b) {
       size_t off = out.blocks_start[s * nb + b];
       for (uint32_t pid : bp[b]) {
+        out.part_ptrs.push_back(parts[s][pid]);
+        out.part_major_stage.push_back((uint32_t)s);
         uint8_t x = opt.xprop ? xflag[s][pid] : 0;
         if (opt.xprop) {
           out.blocks_data[off + 8] = x;

@@ -77,12 +77,18 @@ bool build_partition(const AIG &g, const StagedAIG &st,
                      const std::vector<uint32_t> &endpoints, Partition &out,
                      const PackOptions &opt);
 
+struct CostModel;
+
 // ---------------------------------------------------------------- partitioner
 struct PartitionOptions {
   uint32_t target_cone = 3000;     // AND nodes per initial chunk
   uint32_t target_endpoint_bits = 2048;
   int num_threads = 0;             // 0 = hardware concurrency
   int merge_passes = 1;
+  // when set, merges are accepted on predicted kernel time instead of the
+  // stage-count rule
+  const CostModel *cost_model = nullptr;
+  const std::vector<uint8_t> *xpins = nullptr;
 };
 std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
                                        const PartitionOptions &opt);
@@ -111,6 +117,10 @@ struct FlatScript {
   std::vector<uint32_t> delay_patch_pins;
   // DFF constraints (one per DFF): position of D in state, effective values
   std::vector<uint32_t> dff_data_pos;
+  // the partitions in script order (major stage, block, position), pointing
+  // into the caller's partition vectors
+  std::vector<const Partition *> part_ptrs;
+  std::vector<uint32_t> part_major_stage;
 };
 struct FlattenOptions {
   size_t num_blocks = 148;
@@ -123,6 +133,23 @@ bool flatten_script(const AIG &g, const std::vector<StagedAIG> &stageds,
 // src/flatten.rs:1812-1846: per-thread-position max gate delay into padding.
 void inject_timing(FlatScript &s, const std::vector<uint32_t> &rise,
                    const std::vector<uint32_t> &fall);
+
+// ---------------------------------------------------------------- cost model
+// Partition features for the learned cost model (24 per partition); computed
+// identically for built partitions (training) and merge candidates.
+constexpr int NFEAT = 24;
+void partition_features(const AIG &g, const StagedAIG &st, const Partition &p,
+                        const std::vector<uint8_t> *xpins, float *f);
+
+// A small MLP (NFEAT -> 128 -> 128 -> 1, ReLU) evaluated on the host with
+// bf16-rounded weights and fp32 accumulation; predicts log(kernel cycles).
+struct CostModel {
+  std::vector<float> w1, b1, w2, b2, w3;  // row-major [out][in]
+  float b3 = 0;
+  std::vector<float> mean, inv_std;       // feature normalisation
+  bool valid() const { return !w1.empty(); }
+  float predict(const float *feat) const;
+};
 
 // ---------------------------------------------------------------- checker
 // Walks blocks_data the way the kernel does and checks every index against

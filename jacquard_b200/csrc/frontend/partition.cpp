@@ -17,6 +17,7 @@
 #include "frontend.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <deque>
 #include <stdexcept>
@@ -181,8 +182,23 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
       std::vector<uint32_t> eps = good[i].endpoints;
       eps.insert(eps.end(), good[i + 1].endpoints.begin(), good[i + 1].endpoints.end());
       Partition p;
-      if (build_partition(g, st, eps, p, po) &&
-          p.stages.size() <= std::max(good[i].stages.size(), good[i + 1].stages.size())) {
+      if (!build_partition(g, st, eps, p, po)) return;
+      bool accept;
+      if (opt.cost_model && opt.cost_model->valid()) {
+        // learned rule: merge when the predicted kernel time of the merged
+        // partition is below the two it replaces
+        float fa[NFEAT], fb[NFEAT], fm[NFEAT];
+        partition_features(g, st, good[i], opt.xpins, fa);
+        partition_features(g, st, good[i + 1], opt.xpins, fb);
+        partition_features(g, st, p, opt.xpins, fm);
+        const double ca = std::exp((double)opt.cost_model->predict(fa));
+        const double cb = std::exp((double)opt.cost_model->predict(fb));
+        const double cm = std::exp((double)opt.cost_model->predict(fm));
+        accept = cm < ca + cb;
+      } else {
+        accept = p.stages.size() <= std::max(good[i].stages.size(), good[i + 1].stages.size());
+      }
+      if (accept) {
         trial[i] = std::move(p);
         tok[i] = 1;
       }

@@ -2,9 +2,11 @@
 // run the same script in one launch.
 //
 // Layout: a lane word is one u32 holding one signal of 32 streams.  The state
-// is signal-major, T[signal * L + lane] for L lane words (32*L streams), where
-// `signal` is the bit position of the plain layout (word*32 + bit); the X
-// plane sits at signal offset xoff*32 exactly as in the plain layout.  In this
+// is lane-major, T[lane * signals + signal] for L lane words (32*L streams),
+// where `signal` is the bit position of the plain layout (word*32 + bit); the
+// X plane sits at signal offset xoff*32 exactly as in the plain layout.  A
+// work item touches one lane, so its commit writes are contiguous and the
+// signals one global-read mask selects share a 128-byte line.  In this
 // form the boomerang 16-pair bit shuffle becomes a word gather and every tree
 // position evaluates one 32-stream word:
 //     v[p] = (v[p+L] ^ xa_p) & ((v[p+2L] ^ xb_p) | ob_p),  L = msb(p)
@@ -39,14 +41,20 @@ struct BatchParams {
   size_t sram_words;
   size_t num_cycles;
   size_t sig_per_snap;      // effective words * 32
-  uint32_t *state_a, *state_b;  // ping-pong snapshots, signal-major
-  const uint32_t *stim;     // [cycle+1][input_sigs][lanes] input values, or null
-  size_t input_sigs;        // input region signals (states_start * 32)
+  uint32_t *state_a, *state_b;  // ping-pong snapshots, lane-major
+  const uint32_t *stim;     // [cycle+1][lanes][input_sigs] input values, or null
+  size_t input_sigs;        // stimulus signals per lane per cycle
+  const uint32_t *input_regions;  // (dst signal, src signal, count) triples or null
+  uint32_t n_input_regions;
   const uint32_t *po_sig;   // signals recorded per cycle
   uint32_t n_po;
   uint32_t *wave;           // [cycle][n_po][lanes]
-  uint32_t *record;         // optional full snapshots [cycle+1][sig][lanes]
+  uint32_t *record;         // optional full snapshots [cycle+1][lanes][sig]
   uint32_t wo_slots;        // max num_ios over the script (wo capacity)
+  const uint32_t *block_list;        // non-empty blocks per major stage, or null
+  const uint32_t *block_list_start;  // num_major_stages + 1 offsets
+  unsigned long long *part_cycles;   // optional per-partition SM-clock totals
+  const uint32_t *part_base;         // first partition index of (stage, block)
   uint64_t timeout;
   int slot;
 };
@@ -93,6 +101,10 @@ __device__ __forceinline__ uint32_t perm_at(const uint32_t *chunk, uint32_t q) {
   const uint32_t w = chunk[(k >> 3) * 1024 + T * 4 + ((k >> 1) & 3)];
   return (k & 1) ? (w >> 16) : (w & 0xffffu);
 }
+// Tree-state address of position p in shared memory: a bijective XOR
+// swizzle that gives the 32 lanes of a warp distinct banks under the
+// residue ownership map (lane bits sit at position bits 4..8).
+__device__ __forceinline__ uint32_t sw(uint32_t p) { return p ^ ((p >> 4) & 31u); }
 __device__ __forceinline__ uint32_t bitmask(uint32_t word, uint32_t q) {
   return 0u - ((word >> (q & 31)) & 1u);
 }
@@ -105,15 +117,19 @@ struct Shared {
 };
 
 // One (block, lane) work item: the block's partition list for one lane word.
-__device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t *SX, uint32_t *WO,
-                         uint32_t *WOX, uint32_t *chunks, uint32_t &uses0, uint32_t &uses1,
-                         const uint32_t *script, const uint32_t *in, uint32_t *out, uint32_t lane,
+// Tree state S and writeouts WO hold (value, X) pairs so one shared-memory
+// access moves both lanes; flags are read as one uint4 (xa, xb, ob, delay).
+__device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, uint32_t *chunks,
+                         uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
+                         const uint32_t *in, uint32_t *out, uint32_t lane, uint32_t pid0,
                          bool &failed) {
   const int t = threadIdx.x;
-  const uint32_t L = P.lanes;
+  const size_t lane_base = (size_t)lane * P.sig_per_snap;
   size_t off = 0;
+  uint32_t pid = pid0;
   for (;;) {
     __syncthreads();
+    const long long t_start = clock64();
     if (t < 256) sh.meta[t] = __ldg(script + off + t);
     __syncthreads();
     const uint32_t ns = sh.meta[0];
@@ -133,18 +149,19 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
       tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
     }
 
-    // ---- global read, in two phases so that the loads overlap:
+    // ---- global read, in two phases so that the loads overlap (hooks of the
+    // previous partition read S before this point: the loop-top barrier):
     // (a) thread t < 256 enumerates its (idx, mask) bits and stores, at the
     //     destination position, the source signal (bit 31 = current-cycle
     //     staged IO) or NONE for the unfilled tail; positions follow the
     //     kernel's append order (first appended bit ends up most significant);
     // (b) all threads load their 16 positions with independent loads.
+    uint32_t *Sv = reinterpret_cast<uint32_t *>(S);  // staging: .x words
     if (t < 256) {
-      // all (idx, mask) pairs of this thread in flight at once (R <= 16 in
-      // registers; longer lists are read a second time from global)
       uint2 pr[16];
 #pragma unroll
-      for (int r = 0; r < 16; ++r) pr[r] = (uint32_t)r < R ? ldg2(gr + 512 * r + 2 * t) : make_uint2(0, 0);
+      for (int r = 0; r < 16; ++r)
+        pr[r] = (uint32_t)r < R ? ldg2(gr + 512 * r + 2 * t) : make_uint2(0, 0);
       uint32_t total = 0;
 #pragma unroll
       for (int r = 0; r < 16; ++r) total += __popc(pr[r].y);
@@ -158,7 +175,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
         while (m) {
           const uint32_t k = __ffs(m) - 1;
           m &= m - 1;
-          S[32 * t + (total - 1 - i)] = stg | (w * 32 + k);
+          Sv[2 * sw(32 * t + (total - 1 - i))] = stg | (w * 32 + k);
           ++i;
         }
       }
@@ -170,41 +187,45 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
         while (m) {
           const uint32_t k = __ffs(m) - 1;
           m &= m - 1;
-          S[32 * t + (total - 1 - i)] = stg | (w * 32 + k);
+          Sv[2 * sw(32 * t + (total - 1 - i))] = stg | (w * 32 + k);
           ++i;
         }
       }
-      for (uint32_t k = total; k < 32; ++k) S[32 * t + k] = 0xffffffffu;
+      for (uint32_t k = total; k < 32; ++k) Sv[2 * sw(32 * t + k)] = 0xffffffffu;
     }
     __syncthreads();
     {
       uint32_t e[16], v[16], vx[16];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) e[k] = S[t + BT * k];
+      for (int k = 0; k < 16; ++k) e[k] = Sv[2 * sw(t + BT * k)];
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
         v[k] = 0;
         vx[k] = 0;
         if (e[k] != 0xffffffffu) {
           const uint32_t *base = (e[k] >> 31) ? out : in;
-          const size_t sg = (size_t)(e[k] & 0x7fffffffu) * L + lane;
+          const size_t sg = lane_base + (e[k] & 0x7fffffffu);
           v[k] = ldcg(base + sg);
-          if (is_x) vx[k] = ldcg(base + (size_t)xsig * L + sg);
+          if (is_x) vx[k] = ldcg(base + xsig + sg);
         }
       }
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        S[t + BT * k] = v[k];
-        SX[t + BT * k] = vx[k];
-      }
+      for (int k = 0; k < 16; ++k) S[sw(t + BT * k)] = make_uint2(v[k], vx[k]);
     }
 
+    // Thread -> tree residue map: thread (warp w, lane l) owns positions whose
+    // value mod 512 is u = w | l << 4.  Levels 1..4 then read only the
+    // thread's own registers, levels 5..9 read lanes of the same warp
+    // (residue bits 4..8 are lane bits), and only positions 1..15 need one
+    // exchange through shared memory.
+    const uint32_t lane_i = t & 31, warp_i = t >> 5;
+    const uint32_t u = warp_i | (lane_i << 4);
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
       const uint32_t b = ci & 1;
       uint32_t *C = chunks + b * STAGE_WORDS;
-      // prefetch the next chunk into the other buffer (its last reader
-      // finished before the __syncthreads that ended chunk ci-1)
-      __syncthreads();
+      // The other buffer's last reader finished before the final barrier of
+      // the previous chunk, so the next chunk can be issued right away.
+      if (ci == 0) __syncthreads();
       if (t == 0 && ci + 1 < nchunks) {
         mbar_expect_tx(&sh.bar[b ^ 1], CHUNK_BYTES);
         tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * (ci + 1),
@@ -224,112 +245,108 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
         failed = true;
         return;
       }
-      const uint32_t *F = C + 4096;  // flags: xa, xb, ob, pad per word
+      const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);  // xa, xb, ob, pad
+#define JQ_FL(p, XA, XB, OB)                    \
+  const uint4 fl_##XA = F4[(p) >> 5];           \
+  const uint32_t XA = bitmask(fl_##XA.x, (p));  \
+  const uint32_t XB = bitmask(fl_##XA.y, (p));  \
+  const uint32_t OB = bitmask(fl_##XA.z, (p));
 
       if (ci < ns) {
         // ---------------- boomerang stage ci
         // level 1 (positions 4096 + j): gather both inputs into registers
-        uint32_t va[8], vb[8], xa_[8], xb_[8];
+        uint2 ga[8], gb[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-          const uint32_t j = t + 512 * k;
-          const uint32_t pa = perm_at(C, j), pb = perm_at(C, j + 4096);
-          va[k] = S[pa];
-          vb[k] = S[pb];
-          xa_[k] = is_x ? SX[pa] : 0u;
-          xb_[k] = is_x ? SX[pb] : 0u;
+          const uint32_t j = u + 512 * k;
+          ga[k] = S[sw(perm_at(C, j))];
+          gb[k] = S[sw(perm_at(C, j + 4096))];
         }
         __syncthreads();  // all gathers done before the in-place overwrite
         uint32_t v1[8], x1[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-          const uint32_t p = 4096 + t + 512 * k;
-          const uint32_t fw = (p >> 5) * 4;
-          const uint32_t XA = bitmask(F[fw], p), XB = bitmask(F[fw + 1], p), OB = bitmask(F[fw + 2], p);
-          xand(va[k], xa_[k], vb[k], xb_[k], XA, XB, OB, v1[k], x1[k]);
-          S[p] = v1[k];
-          SX[p] = is_x ? x1[k] : 0u;
+          const uint32_t p = 4096 + u + 512 * k;
+          JQ_FL(p, XA, XB, OB)
+          xand(ga[k].x, ga[k].y, gb[k].x, gb[k].y, XA, XB, OB, v1[k], x1[k]);
+          if (!is_x) x1[k] = 0;
+          S[sw(p)] = make_uint2(v1[k], x1[k]);
         }
-        // level 2: positions 2048 + t + 512k from level-1 k and k+4
         uint32_t v2[4], x2[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          const uint32_t p = 2048 + t + 512 * k;
-          const uint32_t fw = (p >> 5) * 4;
-          xand(v1[k], x1[k], v1[k + 4], x1[k + 4], bitmask(F[fw], p), bitmask(F[fw + 1], p),
-               bitmask(F[fw + 2], p), v2[k], x2[k]);
-          S[p] = v2[k];
-          SX[p] = is_x ? x2[k] : 0u;
+          const uint32_t p = 2048 + u + 512 * k;
+          JQ_FL(p, XA, XB, OB)
+          xand(v1[k], x1[k], v1[k + 4], x1[k + 4], XA, XB, OB, v2[k], x2[k]);
+          if (!is_x) x2[k] = 0;
+          S[sw(p)] = make_uint2(v2[k], x2[k]);
         }
         uint32_t v3[2], x3[2];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          const uint32_t p = 1024 + t + 512 * k;
-          const uint32_t fw = (p >> 5) * 4;
-          xand(v2[k], x2[k], v2[k + 2], x2[k + 2], bitmask(F[fw], p), bitmask(F[fw + 1], p),
-               bitmask(F[fw + 2], p), v3[k], x3[k]);
-          S[p] = v3[k];
-          SX[p] = is_x ? x3[k] : 0u;
+          const uint32_t p = 1024 + u + 512 * k;
+          JQ_FL(p, XA, XB, OB)
+          xand(v2[k], x2[k], v2[k + 2], x2[k + 2], XA, XB, OB, v3[k], x3[k]);
+          if (!is_x) x3[k] = 0;
+          S[sw(p)] = make_uint2(v3[k], x3[k]);
         }
+        uint32_t v4, x4;
         {
-          const uint32_t p = 512 + t;
-          const uint32_t fw = (p >> 5) * 4;
-          uint32_t v4, x4;
-          xand(v3[0], x3[0], v3[1], x3[1], bitmask(F[fw], p), bitmask(F[fw + 1], p),
-               bitmask(F[fw + 2], p), v4, x4);
-          S[p] = v4;
-          SX[p] = is_x ? x4 : 0u;
+          const uint32_t p = 512 + u;
+          JQ_FL(p, XA, XB, OB)
+          xand(v3[0], x3[0], v3[1], x3[1], XA, XB, OB, v4, x4);
+          if (!is_x) x4 = 0;
+          S[sw(p)] = make_uint2(v4, x4);
+        }
+        // level 5: position u (lanes 16..31) from level-4 u-256 (lane ^ 16) and u
+        uint32_t cv, cx;
+        {
+          const uint32_t a = __shfl_xor_sync(0xffffffffu, v4, 16);
+          const uint32_t ax = __shfl_xor_sync(0xffffffffu, x4, 16);
+          const uint32_t p = u;
+          JQ_FL(p & 511, XA, XB, OB)
+          xand(a, ax, v4, x4, XA, XB, OB, cv, cx);
+          if (!is_x) cx = 0;
+          if (lane_i >= 16) S[sw(p)] = make_uint2(cv, cx);
+        }
+        // levels 6..9: the parent of residue u with lane bit k set (lanes
+        // [2^k, 2^(k+1))) reads lanes l + 2^k and l + 2^(k+1)
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+          const uint32_t d = 1u << k;
+          const uint32_t a = __shfl_sync(0xffffffffu, cv, (lane_i + d) & 31);
+          const uint32_t bb = __shfl_sync(0xffffffffu, cv, (lane_i + 2 * d) & 31);
+          const uint32_t ax = __shfl_sync(0xffffffffu, cx, (lane_i + d) & 31);
+          const uint32_t bx = __shfl_sync(0xffffffffu, cx, (lane_i + 2 * d) & 31);
+          if (lane_i >= d && lane_i < 2 * d) {
+            const uint32_t p = u;
+            JQ_FL(p, XA, XB, OB)
+            xand(a, ax, bb, bx, XA, XB, OB, cv, cx);
+            if (!is_x) cx = 0;
+            S[sw(p)] = make_uint2(cv, cx);
+          }
         }
         __syncthreads();
-        // levels 5..7 in shared memory (256, 128, 64 positions)
-#pragma unroll
-        for (uint32_t len = 256; len >= 64; len >>= 1) {
-          if ((uint32_t)t < len) {
-            const uint32_t p = len + t;
-            const uint32_t fw = (p >> 5) * 4;
-            uint32_t r, rx;
-            xand(S[p + len], SX[p + len], S[p + 2 * len], SX[p + 2 * len], bitmask(F[fw], p),
-                 bitmask(F[fw + 1], p), bitmask(F[fw + 2], p), r, rx);
-            S[p] = r;
-            SX[p] = is_x ? rx : 0u;
-          }
-          __syncthreads();
-        }
-        // levels 8..13 (positions 32..63 down to 1) inside warp 0
+        // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
         if (t < 32) {
-          const uint32_t fw0 = 4 * 0, fw1 = 4 * 1;
-          uint32_t cur, curx;
-          {
-            const uint32_t p = 32 + t;
-            xand(S[p + 32], SX[p + 32], S[p + 64], SX[p + 64], bitmask(F[fw1], p),
-                 bitmask(F[fw1 + 1], p), bitmask(F[fw1 + 2], p), cur, curx);
-            if (!is_x) curx = 0;
-            S[p] = cur;
-            SX[p] = curx;
-          }
-          // lane i holds position 2*len + i of the previous level; position
-          // len + i reads 2*len + i (own) and 3*len + i (lane i + len)
-          uint32_t hv = cur, hx = curx;
+          uint2 h = t < 16 ? S[sw(16 + t)] : make_uint2(0, 0);
+          uint32_t hv = h.x, hx = h.y;
 #pragma unroll
-          for (uint32_t len = 16; len >= 1; len >>= 1) {
+          for (uint32_t len = 8; len >= 1; len >>= 1) {
             const uint32_t bb = __shfl_sync(0xffffffffu, hv, (t + len) & 31);
             const uint32_t bx = __shfl_sync(0xffffffffu, hx, (t + len) & 31);
             if ((uint32_t)t < len) {
               const uint32_t p = len + t;
+              JQ_FL(p, XA, XB, OB)
               uint32_t r, rx;
-              xand(hv, hx, bb, bx, bitmask(F[fw0], p), bitmask(F[fw0 + 1], p),
-                   bitmask(F[fw0 + 2], p), r, rx);
+              xand(hv, hx, bb, bx, XA, XB, OB, r, rx);
               if (!is_x) rx = 0;
-              S[p] = r;
-              SX[p] = rx;
+              S[sw(p)] = make_uint2(r, rx);
               hv = r;
               hx = rx;
             }
           }
-          if (t == 0) {
-            S[0] = 0;
-            SX[0] = 0;
-          }
+          if (t == 0) S[0] = make_uint2(0, 0);
         }
         __syncthreads();
         // writeout hooks of this stage
@@ -337,38 +354,35 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
           const uint32_t slot = q >> 5;
           const uint32_t hw = sh.meta[128 + slot / 2];
           const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
-          if ((hook >> 8) == ci) {
-            const uint32_t src = (hook & 255u) * 32 + (q & 31);
-            WO[q] = S[src];
-            WOX[q] = SX[src];
-          }
+          if ((hook >> 8) == ci) WO[q] = S[sw((hook & 255u) * 32 + (q & 31))];
         }
       } else if (ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
         // stage the permuted words in S (free now: all hooks are done)
         for (uint32_t q = t; q < nq; q += BT) {
-          const uint32_t src = perm_at(C, q);
-          const uint32_t inv = bitmask(F[(q >> 5) * 4], q), set0 = bitmask(F[(q >> 5) * 4 + 1], q);
-          S[q] = (WO[src] & ~set0) ^ inv;
-          SX[q] = is_x ? (WOX[src] & ~set0) : 0u;
+          const uint2 w = WO[perm_at(C, q)];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q);
+          S[q] = make_uint2((w.x & ~set0) ^ inv, is_x ? (w.y & ~set0) : 0u);
         }
         __syncthreads();
         // one warp per SRAM, lane = stream within the lane word
         const int warp = t >> 5, ln = t & 31;
         for (uint32_t i = warp; i < num_srams; i += BT / 32) {
-          const uint32_t *A = S + (4 * i) * 32;
+          const uint2 *A = S + (4 * i) * 32;
           uint32_t ra = 0, wa = 0, en = 0, data = 0, datax = 0;
 #pragma unroll
           for (int k = 0; k < 16; ++k) {
-            ra |= ((A[k] >> ln) & 1u) << k;
-            wa |= ((A[16 + k] >> ln) & 1u) << k;
+            ra |= ((A[k].x >> ln) & 1u) << k;
+            wa |= ((A[16 + k].x >> ln) & 1u) << k;
           }
 #pragma unroll 8
           for (int k = 0; k < 32; ++k) {
-            en |= ((A[32 + k] >> ln) & 1u) << k;
-            data |= ((A[64 + k] >> ln) & 1u) << k;
-            datax |= ((SX[(4 * i + 2) * 32 + k] >> ln) & 1u) << k;
+            en |= ((A[32 + k].x >> ln) & 1u) << k;
+            const uint2 dk = A[64 + k];
+            data |= ((dk.x >> ln) & 1u) << k;
+            datax |= ((dk.y >> ln) & 1u) << k;
           }
           const size_t stream = (size_t)lane * 32 + ln;
           uint32_t *ram = P.sram + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS;
@@ -390,17 +404,12 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
           for (int k = 0; k < 32; ++k) {
             const uint32_t word = __ballot_sync(0xffffffffu, (r >> k) & 1u);
             const uint32_t wordx = __ballot_sync(0xffffffffu, (rx >> k) & 1u);
-            if (ln == k) {
-              WO[slotw + k] = word;
-              WOX[slotw + k] = is_x ? wordx : 0u;
-            }
+            if (ln == k) WO[slotw + k] = make_uint2(word, is_x ? wordx : 0u);
           }
         }
-        for (uint32_t q = t; q < num_dup * 32; q += BT) {
-          const uint32_t dst = (num_ios - num_srams - num_dup) * 32 + q;
-          WO[dst] = S[num_srams * 4 * 32 + q];
-          WOX[dst] = SX[num_srams * 4 * 32 + q];
-        }
+        for (uint32_t q = t; q < num_dup * 32; q += BT)
+          WO[(num_ios - num_srams - num_dup) * 32 + q] = S[num_srams * 4 * 32 + q];
+        __syncthreads();
       } else {
         // ---------------- clock-enable permutation and commit (4 words per
         // thread in flight)
@@ -409,36 +418,45 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
           uint32_t cp[4], cpx[4], wv[4], wx[4], old[4], oldx[4];
           size_t sg[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const uint32_t q = q0 + u * BT;
+          for (int uu = 0; uu < 4; ++uu) {
+            const uint32_t q = q0 + uu * BT;
             if (q < nq) {
-              const uint32_t src = perm_at(C, q);
-              const uint32_t fw = (q >> 5) * 4;
-              const uint32_t inv = bitmask(F[fw], q), set0 = bitmask(F[fw + 1], q),
-                             dinv = bitmask(F[fw + 2], q);
-              cp[u] = (WO[src] & ~set0) ^ inv;
-              cpx[u] = is_x ? (WOX[src] & ~set0) : 0u;
-              wv[u] = WO[q] ^ dinv;
-              wx[u] = WOX[q];
-              sg[u] = ((size_t)io_off * 32 + q) * L + lane;
-              old[u] = ldcg(in + sg[u]);
-              oldx[u] = is_x ? ldcg(in + (size_t)xsig * L + sg[u]) : 0u;
+              const uint2 src = WO[perm_at(C, q)];
+              const uint4 fl = F4[q >> 5];
+              const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q),
+                             dinv = bitmask(fl.z, q);
+              const uint2 me = WO[q];
+              cp[uu] = (src.x & ~set0) ^ inv;
+              cpx[uu] = is_x ? (src.y & ~set0) : 0u;
+              wv[uu] = me.x ^ dinv;
+              wx[uu] = me.y;
+              sg[uu] = lane_base + (size_t)io_off * 32 + q;
+              old[uu] = ldcg(in + sg[uu]);
+              oldx[uu] = is_x ? ldcg(in + xsig + sg[uu]) : 0u;
             }
           }
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const uint32_t q = q0 + u * BT;
+          for (int uu = 0; uu < 4; ++uu) {
+            const uint32_t q = q0 + uu * BT;
             if (q < nq) {
-              out[sg[u]] = (old[u] & ~cp[u]) | (wv[u] & cp[u]);
+              out[sg[uu]] = (old[uu] & ~cp[uu]) | (wv[uu] & cp[uu]);
               if (is_x)
-                out[(size_t)xsig * L + sg[u]] =
-                    (oldx[u] & ~cp[u] & ~cpx[u]) | (wx[u] & cp[u] & ~cpx[u]) | cpx[u];
+                out[xsig + sg[uu]] =
+                    (oldx[uu] & ~cp[uu] & ~cpx[uu]) | (wx[uu] & cp[uu] & ~cpx[uu]) | cpx[uu];
             }
           }
         }
       }
+#undef JQ_FL
     }
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    if (P.part_cycles) {
+      // per-partition kernel time, measured by the simulator itself (the
+      // training signal of the partition cost model)
+      __syncthreads();
+      if (t == 0) atomicAdd(&P.part_cycles[pid], (unsigned long long)(clock64() - t_start));
+    }
+    ++pid;
     if (is_last) break;
   }
 }
@@ -446,46 +464,59 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint32_t *S, uint32_t
 __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   extern __shared__ __align__(128) uint8_t dyn[];
   __shared__ Shared sh;
-  uint32_t *chunks = reinterpret_cast<uint32_t *>(dyn);        // 2 x 20 KB
-  uint32_t *S = chunks + 2 * STAGE_WORDS;                       // 8192
-  uint32_t *SX = S + 8192;                                      // 8192
-  uint32_t *WO = SX + 8192;                                     // wo_slots*32
-  uint32_t *WOX = WO + P.wo_slots * 32;
+  uint32_t *chunks = reinterpret_cast<uint32_t *>(dyn);               // 2 x 20 KB
+  uint2 *S = reinterpret_cast<uint2 *>(chunks + 2 * STAGE_WORDS);      // 8192 (v, x)
+  uint2 *WO = S + 8192;                                               // wo_slots*32
   const int t = threadIdx.x;
   if (t == 0) {
     mbar_init(&sh.bar[0], 1);
     mbar_init(&sh.bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (uint32_t q = t; q < P.wo_slots * 32; q += BT) {
-    WO[q] = 0;
-    WOX[q] = 0;
-  }
+  for (uint32_t q = t; q < P.wo_slots * 32; q += BT) WO[q] = make_uint2(0, 0);
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
   const size_t snap = P.sig_per_snap * P.lanes;
-  const uint32_t items = P.num_blocks * P.lanes;
+
   for (size_t c = 0; c < P.num_cycles; ++c) {
     const uint32_t *in = (c & 1) ? P.state_b : P.state_a;
     uint32_t *out = (c & 1) ? P.state_a : P.state_b;
     // inputs of snapshot c+1 into the output buffer's input region
     if (P.stim) {
+      // stimulus row layout [lane][input_sigs]; each input region copies
+      // stimulus signals [src, src+count) to state signals [dst, dst+count)
+      // (one region at 0 when no list is given)
       const uint32_t *src = P.stim + (c + 1) * P.input_sigs * P.lanes;
       for (size_t q = (size_t)blockIdx.x * BT + t; q < P.input_sigs * P.lanes;
-           q += (size_t)gridDim.x * BT)
-        out[q] = src[q];
+           q += (size_t)gridDim.x * BT) {
+        const size_t l = q / P.input_sigs, i = q % P.input_sigs;
+        size_t dst = i;
+        if (P.input_regions) {
+          for (uint32_t r = 0; r < P.n_input_regions; ++r) {
+            const uint32_t d0 = P.input_regions[3 * r], s0 = P.input_regions[3 * r + 1],
+                           n = P.input_regions[3 * r + 2];
+            if (i >= s0 && i < s0 + n) dst = d0 + (i - s0);
+          }
+        }
+        out[l * P.sig_per_snap + dst] = src[q];
+      }
     }
     for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
+      const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
+                                         : P.num_blocks;
+      const uint32_t items = nblk * P.lanes;
       for (;;) {
         __syncthreads();
         if (t == 0) sh.ticket = atomicAdd(&g_ticket[P.slot], 1u);
         __syncthreads();
         const uint32_t tk = sh.ticket;
         if (tk >= items) break;
-        const uint32_t blk = tk / P.lanes, lane = tk % P.lanes;
+        const uint32_t bi = tk / P.lanes, lane = tk % P.lanes;
+        const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
         const uint32_t *script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
-        run_item(P, sh, S, SX, WO, WOX, chunks, uses0, uses1, script, in, out, lane, failed);
+        const uint32_t pid0 = P.part_base ? P.part_base[(size_t)ms * P.num_blocks + blk] : 0u;
+        run_item(P, sh, S, WO, chunks, uses0, uses1, script, in, out, lane, pid0, failed);
         if (failed) {
           if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
           return;
@@ -524,7 +555,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
     for (size_t q = (size_t)blockIdx.x * BT + t; q < (size_t)P.n_po * P.lanes;
          q += (size_t)gridDim.x * BT) {
       const uint32_t po = (uint32_t)(q / P.lanes), l = (uint32_t)(q % P.lanes);
-      P.wave[(c * P.n_po + po) * P.lanes + l] = ldcg(out + (size_t)P.po_sig[po] * P.lanes + l);
+      P.wave[(c * P.n_po + po) * P.lanes + l] = ldcg(out + (size_t)l * P.sig_per_snap + P.po_sig[po]);
     }
     if (P.record) {
       uint32_t *dst = P.record + (c + 1) * snap;
@@ -539,6 +570,14 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 }  // namespace jqk
 
 using namespace jqk;
+
+// Re-arms one slot's barrier, ticket and status before a launch.  A kernel
+// (not a host copy) so the reset is captured in CUDA graphs with the launch.
+__global__ void jq_batched_reset_kernel(int slot) {
+  g_bar_count[slot] = 0;
+  g_ticket[slot] = 0;
+  g_status[slot] = 0;
+}
 
 extern "C" {
 
@@ -586,22 +625,22 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.state_b = a->state_b;
   P.stim = a->stimulus;
   P.input_sigs = a->input_signals;
+  P.input_regions = a->input_regions;
+  P.n_input_regions = a->n_input_regions;
   P.po_sig = a->po_signals;
   P.n_po = a->n_po;
   P.wave = a->wave;
   P.record = a->record;
   P.wo_slots = a->wo_slots ? a->wo_slots : 256;
+  P.block_list = a->block_list;
+  P.block_list_start = a->block_list_start;
+  P.part_cycles = a->part_cycles;
+  P.part_base = a->part_base;
+  if (P.part_cycles && !P.part_base) return JQ_ERR_INVALID_ARG;
   P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
   P.slot = 1;
-  static const unsigned zero_u[1] = {0};
-  static const int zero_i[1] = {0};
-  if (cudaMemcpyToSymbolAsync(g_bar_count, zero_u, sizeof(unsigned), P.slot * sizeof(unsigned),
-                              cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemcpyToSymbolAsync(g_ticket, zero_u, sizeof(unsigned), P.slot * sizeof(unsigned),
-                              cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemcpyToSymbolAsync(g_status, zero_i, sizeof(int), P.slot * sizeof(int),
-                              cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return JQ_ERR_LAUNCH;
+  jq_batched_reset_kernel<<<1, 1, 0, st>>>(P.slot);
+  if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
   int smem = jq_batched_smem_bytes(P.wo_slots);
   void *args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel((void *)jq_batched_kernel, (unsigned)grid, BT, args,

@@ -295,6 +295,13 @@ using namespace jqk;
 
 namespace {
 
+// Re-arms one slot's barrier and status before a launch (a kernel, so that
+// it is captured in CUDA graphs together with the launch).
+__global__ void jq_plain_reset_kernel(int slot) {
+  g_bar_count[slot] = 0;
+  g_status[slot] = 0;
+}
+
 int g_max_blocks_cache[64];
 
 int launch_plain(const jq_sim_args *a, uint32_t event_cap, int slot) {
@@ -327,14 +334,8 @@ int launch_plain(const jq_sim_args *a, uint32_t event_cap, int slot) {
   P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
   P.slot = slot;
   // reset this slot's barrier (ordered before the kernel on the stream)
-  static const unsigned zero_u[1] = {0};
-  static const int zero_i[1] = {0};
-  if (cudaMemcpyToSymbolAsync(g_bar_count, zero_u, sizeof(unsigned), slot * sizeof(unsigned),
-                              cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return JQ_ERR_LAUNCH;
-  if (cudaMemcpyToSymbolAsync(g_status, zero_i, sizeof(int), slot * sizeof(int),
-                              cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return JQ_ERR_LAUNCH;
+  jq_plain_reset_kernel<<<1, 1, 0, st>>>(slot);
+  if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
   void *args[] = {&P};
   cudaError_t e = track ? cudaLaunchCooperativeKernel((void *)jq_plain_kernel<true>, P.num_blocks,
                                                       NT, args, 0, st)

@@ -13,6 +13,8 @@ import numpy as np
 from ._native import load
 
 c_u32p = ctypes.POINTER(ctypes.c_uint32)
+NFEAT = 24
+COST_MODEL_FLOATS = 128 * 24 + 128 + 128 * 128 + 128 + 128 + 1 + 24 + 24
 
 
 class _GenParams(ctypes.Structure):
@@ -35,7 +37,8 @@ class _BuildParams(ctypes.Structure):
     _fields_ = [("num_blocks", ctypes.c_size_t), ("xprop", ctypes.c_int32),
                 ("n_level_split", ctypes.c_uint32), ("level_split", c_u32p),
                 ("target_cone", ctypes.c_uint32), ("target_endpoint_bits", ctypes.c_uint32),
-                ("num_threads", ctypes.c_int32), ("merge_passes", ctypes.c_int32)]
+                ("num_threads", ctypes.c_int32), ("merge_passes", ctypes.c_int32),
+                ("cost_model", ctypes.c_void_p)]
 
 
 class _ScriptInfo(ctypes.Structure):
@@ -69,6 +72,10 @@ def _lib():
         lib.jqf_constraint_buffer.restype = ctypes.c_int
         lib.jqf_constraint_buffer.argtypes = [u32, ctypes.c_uint64, sz, vp, vp, vp, vp,
                                               ctypes.POINTER(u32), vp]
+        lib.jqf_script_features.restype = ctypes.c_int
+        lib.jqf_script_features.argtypes = [vp, vp, vp]
+        lib.jqf_cost_model_predict.restype = ctypes.c_int
+        lib.jqf_cost_model_predict.argtypes = [vp, vp, sz, vp]
         lib.jqf_inject_delays.restype = ctypes.c_int
         lib.jqf_inject_delays.argtypes = [vp, sz, sz, vp, vp, vp, vp, vp, sz]
         lib._jq_typed = True
@@ -169,20 +176,26 @@ class Design:
             raise ValueError("delay arrays must have num_pins + 1 entries")
 
     def build_script(self, num_blocks=148, xprop=False, level_split=(), target_cone=0,
-                     target_endpoint_bits=0, num_threads=0, merge_passes=1):
+                     target_endpoint_bits=0, num_threads=0, merge_passes=1, cost_model=None):
+        """cost_model: flat float32 array (JQF_COST_MODEL_FLOATS) or None."""
         return Script(self, num_blocks, xprop, level_split, target_cone,
-                      target_endpoint_bits, num_threads, merge_passes)
+                      target_endpoint_bits, num_threads, merge_passes, cost_model)
 
 
 class Script:
     """FlattenedScriptV1: blocks_start / blocks_data plus the state layout."""
 
     def __init__(self, design, num_blocks, xprop, level_split, target_cone,
-                 target_endpoint_bits, num_threads, merge_passes):
+                 target_endpoint_bits, num_threads, merge_passes, cost_model=None):
         lib = _lib()
         ls = (ctypes.c_uint32 * max(1, len(level_split)))(*level_split)
+        cm = None
+        if cost_model is not None:
+            cm = np.ascontiguousarray(cost_model, dtype=np.float32)
+            assert cm.size == COST_MODEL_FLOATS
         bp = _BuildParams(num_blocks, int(bool(xprop)), len(level_split), ls, target_cone,
-                          target_endpoint_bits, num_threads, merge_passes)
+                          target_endpoint_bits, num_threads, merge_passes,
+                          cm.ctypes.data if cm is not None else None)
         err = ctypes.create_string_buffer(512)
         h = lib.jqf_build_script(design._h, ctypes.byref(bp), err, 512)
         if not h:
@@ -217,6 +230,8 @@ class Script:
             self.stage_block_part = arr(9, np.uint32).reshape(-1, 3)
             # (major stage, #boomerang stages, cone ANDs, targets, endpoints)
             self.partition_stats = arr(10, np.uint32).reshape(-1, 5)
+            self.features = np.zeros((self.num_partitions, NFEAT), np.float32)
+            lib.jqf_script_features(design._h, h, self.features.ctypes.data)
         finally:
             lib.jqf_free_script(h)
         self.timing_arrivals_enabled = False

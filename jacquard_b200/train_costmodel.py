@@ -1,0 +1,132 @@
+"""Train the partition cost model on timings measured by the simulator.
+
+  python -m jacquard_b200.train_costmodel [--samples 20000] [--steps 2000]
+         [--out jacquard_b200/models/costmodel.npz] [--eval-clusters 1024]
+
+1. Builds scripts of seeded SoC-family designs (the SoC workload's generator at
+   several sizes and seeds) with varied level splits and partition sizes.
+2. Runs each on the batched interpreter with per-partition timing
+   (`part_cycles`) and records log(mean SM cycles per partition work item)
+   next to the partition's 24 features.
+3. Trains the MLP with Adam (lr 1e-3, batch 512) on the GPU kernels.
+4. Evaluates on a fresh design: heuristic vs learned partitioner, device-timed
+   stimulus-cycles/s of the batched interpreter, same stimulus.
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+import torch
+
+from . import autotune, batched, costmodel, frontend
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def measure(design, split_every, cone, lanes=4, cycles=4, blocks=148, cost_model=None):
+    s = design.build_script(num_blocks=blocks, level_split=tuple(range(split_every, 80, split_every)),
+                            xprop=True, target_cone=cone, cost_model=cost_model)
+    B = batched.BatchedSim(s, lanes)
+    B.load_state(np.zeros((lanes, B.sig), np.uint32))
+    B.reset_sram()
+    pc = torch.zeros(s.num_partitions, dtype=torch.int64, device="cuda")
+    B.run(None, 1)
+    B.run(None, cycles, part_cycles=pc)
+    torch.cuda.synchronize()
+    assert B.status() == 0
+    per_item = pc.cpu().numpy().astype(np.float64) / (lanes * cycles)
+    ok = per_item > 0
+    return s.features[ok], np.log(per_item[ok]).astype(np.float32)
+
+
+def collect(target, seed0=100, log=print):
+    feats, ys = [], []
+    rng = np.random.default_rng(seed0)
+    n = 0
+    k = 0
+    while n < target:
+        clusters = int(rng.choice([32, 64, 128]))
+        d = frontend.Design(frontend.soc_params(seed=seed0 + k, n_clusters=clusters,
+                                                n_dff=200_000 * clusters // 512, n_sram=4))
+        split = int(rng.choice([4, 5, 6, 8, 10]))
+        cone = int(rng.choice([1000, 2000, 4000, 6000, 9000, 12000]))
+        try:
+            f, y = measure(d, split, cone)
+        except RuntimeError as e:
+            log(f"  skip: {e}")
+            k += 1
+            continue
+        feats.append(f)
+        ys.append(y)
+        n += len(y)
+        k += 1
+        log(f"  design {k}: {clusters} clusters, split {split}, cone {cone}: {len(y)} partitions ({n} total)")
+    return np.concatenate(feats)[:target], np.concatenate(ys)[:target]
+
+
+def evaluate(model_packed, clusters=1024, cycles=5000, lanes=8, seed=4242, split=5, cone=6000,
+             log=print):
+    """Heuristic vs learned partitioner on one fresh design: batched
+    stimulus-cycles/s over `cycles` cycles (device time, one launch each)."""
+    d = frontend.Design(frontend.soc_params(seed=seed, n_clusters=clusters,
+                                            n_dff=200_000 * clusters // 512))
+    out = {"design_ands": int(d.num_and), "cycles": cycles, "streams": 32 * lanes}
+    for name, cm in (("heuristic", None), ("learned", model_packed)):
+        t0 = time.perf_counter()
+        s = d.build_script(num_blocks=148, level_split=tuple(range(split, 80, split)), xprop=True,
+                           target_cone=cone, cost_model=cm, merge_passes=3)
+        bt = time.perf_counter() - t0
+        B = batched.BatchedSim(s, lanes)
+        B.load_state(np.zeros((lanes, B.sig), np.uint32))
+        B.reset_sram()
+        B.run(None, 2)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        B.run(None, cycles)
+        e1.record()
+        torch.cuda.synchronize()
+        assert B.status() == 0
+        ms = e0.elapsed_time(e1)
+        out[name] = {"stream_cycles_per_s": 32 * lanes * cycles / (ms / 1e3), "partitions": s.num_partitions,
+                     "script_mb_per_cycle": s.script_words_per_cycle() * 4 / 1e6, "build_s": bt}
+        log(f"  {name}: {out[name]}")
+    out["gain"] = out["learned"]["stream_cycles_per_s"] / out["heuristic"]["stream_cycles_per_s"]
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--samples", type=int, default=20000)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--out", default=os.path.join(HERE, "models", "costmodel.npz"))
+    ap.add_argument("--eval-clusters", type=int, default=1024)
+    ap.add_argument("--eval-cycles", type=int, default=5000)
+    args = ap.parse_args()
+    t0 = time.time()
+    X, y = collect(args.samples)
+    print(f"collected {len(y)} partitions in {time.time() - t0:.0f}s; log-cycles mean {y.mean():.2f} sd {y.std():.2f}")
+    perm = np.random.default_rng(0).permutation(len(y))
+    ntr = int(0.9 * len(y))
+    tr, te = perm[:ntr], perm[ntr:]
+    m = costmodel.CostModel(seed=5)
+    hist = m.fit(X[tr], y[tr], steps=args.steps, batch=512, lr=1e-3)
+    pred = m.predict(X[te])
+    mse = float(np.mean((pred - y[te]) ** 2))
+    base = float(np.var(y[te]))
+    print(f"train loss {hist[0][1]:.3f} -> {hist[-1][1]:.3f}; held-out mse {mse:.4f} (variance {base:.4f}, R^2 {1 - mse / base:.3f})")
+    m.save(args.out)
+    ev = evaluate(m.pack(), clusters=args.eval_clusters, cycles=args.eval_cycles)
+    summary = {"samples": int(len(y)), "steps": args.steps, "loss_start": hist[0][1],
+               "loss_end": hist[-1][1], "heldout_mse": mse, "heldout_var": base,
+               "heldout_r2": 1 - mse / base, "eval": ev}
+    with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
+        json.dump(summary, f, indent=1)
+    print(json.dumps(summary))
+
+
+if __name__ == "__main__":
+    main()

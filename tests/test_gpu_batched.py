@@ -40,15 +40,15 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes):
         wsram.append(sram)
     # batched
     B = batched.BatchedSim(s, lanes, record=True)
-    bt = batched.to_batched(snaps)  # (cycles+1, sig, lanes)
+    bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
     B.load_state(bt[0])
     B.reset_sram()
-    stim = torch.from_numpy(np.ascontiguousarray(bt[:, :B.in_sigs, :]).reshape(-1).view(np.int32)).cuda()
+    stim = torch.from_numpy(np.ascontiguousarray(bt[:, :, :B.in_sigs]).reshape(-1).view(np.int32)).cuda()
     rec = torch.zeros((cycles + 1) * B.sig * lanes, dtype=torch.int32, device="cuda")
     rec[: B.sig * lanes].copy_(torch.from_numpy(np.ascontiguousarray(bt[0]).reshape(-1).view(np.int32)))
     B.run(stim, cycles, record_buf=rec)
     assert B.status() == 0
-    got = batched.from_batched(rec.cpu().numpy().view(np.uint32).reshape(cycles + 1, B.sig, lanes), eff)
+    got = batched.from_batched(rec.cpu().numpy().view(np.uint32).reshape(cycles + 1, lanes, B.sig), eff)
     assert got.shape == want.shape
     for k in range(S):
         assert np.array_equal(got[k], want[k]), f"stream {k}"
@@ -61,3 +61,49 @@ def test_layout_roundtrip():
     rng = np.random.default_rng(0)
     a = rng.integers(0, 2**32, size=(64, 3, 5), dtype=np.uint64).astype(np.uint32)
     assert np.array_equal(batched.from_batched(batched.to_batched(a), 5), a)
+
+
+def _batched_inputs(kind, s, cycles, lanes, seed0):
+    S = 32 * lanes
+    snaps = np.stack([cases.stimulus(kind, s, cycles, seed=seed0 + k, x_init=True) for k in range(S)])
+    return batched.to_batched(snaps)  # (cycles+1, lanes, sig)
+
+
+def test_multi_design_single_launch_matches_separate_runs():
+    """Three designs of uneven size relocated into one script share one
+    persistent launch; each design's state equals its own separate run."""
+    specs = [("tiny", 8, (5,)), ("sram", 16, (8,)), ("soc_mini", 148, (20, 40, 60))]
+    scripts = [cases.script(k, nb, sp, xprop=True) for k, nb, sp in specs]
+    lanes, cycles = 1, 8
+    bts = [_batched_inputs(k, s, cycles, lanes, 500 + 37 * i)
+           for i, ((k, _, _), s) in enumerate(zip(specs, scripts))]
+    finals = []
+    for s, bt in zip(scripts, bts):
+        B = batched.BatchedSim(s, lanes)
+        B.load_state(bt[0])
+        B.reset_sram()
+        stim = torch.from_numpy(np.ascontiguousarray(bt[:, :, :B.in_sigs]).reshape(-1).view(np.int32)).cuda()
+        B.run(stim, cycles)
+        assert B.status() == 0
+        finals.append(B.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, -1))
+    C = batched.CombinedScript(scripts)
+    BC = batched.BatchedSim(C, lanes)
+    snap0 = np.concatenate([bt[0] for bt in bts], axis=-1)
+    assert snap0.shape == (lanes, BC.sig)
+    BC.load_state(snap0)
+    BC.reset_sram()
+    stim = np.concatenate([bt[:, :, :batched.input_words(s) * 32] for s, bt in zip(scripts, bts)], axis=-1)
+    stim_d = torch.from_numpy(np.ascontiguousarray(stim).reshape(-1).view(np.int32)).cuda()
+    # capture the launch in a CUDA graph and replay it
+    g = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        BC.run(stim_d, cycles)
+    g.replay()
+    torch.cuda.synchronize()
+    assert BC.status() == 0
+    got = BC.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, -1)
+    for d, s in enumerate(scripts):
+        lo = C.state_base[d] * 32
+        n = 2 * s.reg_io_state_size * 32
+        assert np.array_equal(got[:, lo:lo + n], finals[d]), f"design {d}"
