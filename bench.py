@@ -99,9 +99,21 @@ def build_design(seed=2, clusters=512, n_dff=200_000):
     return d
 
 
-def build_script(d, num_blocks, xprop=True):
+MODEL_PATH = os.path.join(HERE, "jacquard_b200", "trained", "costmodel.npz")
+
+
+def learned_model():
+    """The trained partition cost model (jacquard_b200/trained), or None."""
+    if not os.path.exists(MODEL_PATH):
+        return None
+    from jacquard_b200 import costmodel
+    return costmodel.packed_from_file(MODEL_PATH)
+
+
+def build_script(d, num_blocks, xprop=True, cost_model=None):
     return d.build_script(num_blocks=num_blocks, level_split=LEVEL_SPLIT, xprop=xprop,
-                          target_cone=TARGET_CONE)
+                          target_cone=TARGET_CONE, cost_model=cost_model,
+                          merge_passes=3 if cost_model is not None else 1)
 
 
 def algorithmic_bytes_per_cycle(s, lanes=1, arrivals=False):
@@ -226,7 +238,8 @@ def run_mine_batched(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
-    s = build_script(d, args.blocks)
+    model = None if args.no_learned else learned_model()
+    s = build_script(d, args.blocks, cost_model=model)
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
@@ -283,8 +296,38 @@ def run_mine_batched(args, rank, world):
                 launches_per_step=1,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
-                            major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes),
+                            major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
+                            partitioner="learned" if model is not None else "heuristic"),
                 script=s, d=d)
+
+
+def compare_kernels(d, args, window=16, reps=3):
+    """Single-stream cycles/s of the plain interpreter (reference state layout,
+    one stimulus stream) on a script of the same design, built for 296
+    blocks: the grid the reference's kernel fits at 2 CTAs per SM."""
+    import torch
+    from jacquard_b200 import sim
+    s = build_script(d, 296)
+    eff = 2 * s.reg_io_state_size
+    host = stimulus_window(s, d, 0, window, seed=100)
+    ds = sim.DeviceScript(s)
+    st = sim.u32_to_dev(host.reshape(-1))
+    n_sram = max(1, s.sram_storage_size)
+    sram = torch.zeros(n_sram, dtype=torch.int32, device="cuda")
+    sram_x = torch.full((n_sram,), -1, dtype=torch.int32, device="cuda")
+    out = {"window": window, "blocks": 296}
+    fn = lambda: sim.simulate(ds, st, window, eff, sram, sram_x)
+    fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    out["plain_kernel"] = {"cycles_per_s": window * reps / (e0.elapsed_time(e1) / 1e3), "streams": 1}
+    return out
 
 
 def cpu_baseline(s, d, cycles=8, threads=1):
@@ -315,6 +358,9 @@ def main():
     ap.add_argument("--clusters", type=int, default=512,
                     help="design size in 4096-gate clusters (512 = the 2M-gate workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-learned", action="store_true", help="heuristic partitioner only")
+    ap.add_argument("--compare", action="store_true",
+                    help="also time the single-stream plain kernel on the same design")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -389,6 +435,8 @@ def main():
                         "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
                 "gpu_launches": r["launches_per_step"] * args.steps,
                 "clocks": r["clocks"]}
+        if args.compare and args.mode == "batched":
+            line["compare"] = compare_kernels(r["d"], args)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -1,7 +1,7 @@
 """Train the partition cost model on timings measured by the simulator.
 
   python -m jacquard_b200.train_costmodel [--samples 20000] [--steps 2000]
-         [--out jacquard_b200/models/costmodel.npz] [--eval-clusters 1024]
+         [--out jacquard_b200/trained/costmodel.npz] [--eval-clusters 1024]
 
 1. Builds scripts of seeded SoC-family designs (the SoC workload's generator at
    several sizes and seeds) with varied level splits and partition sizes.
@@ -102,7 +102,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--out", default=os.path.join(HERE, "models", "costmodel.npz"))
+    ap.add_argument("--out", default=os.path.join(HERE, "trained", "costmodel.npz"))
     ap.add_argument("--eval-clusters", type=int, default=1024)
     ap.add_argument("--eval-cycles", type=int, default=5000)
     args = ap.parse_args()

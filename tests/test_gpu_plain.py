@@ -133,3 +133,48 @@ def test_reference_kernel_matches_oracle(xprop):
     got = sim.dev_to_u32(st).reshape(states.shape)
     assert np.array_equal(got, want)
     assert np.array_equal(sim.dev_to_u32(sram)[:wsram.size], wsram)
+
+
+def test_windowed_timed_run_drains_every_violation():
+    """Timed path over several launch windows with per-window event drains
+    (the CUDA timed path the reference never wired) vs the oracle run with
+    the same windows."""
+    from jacquard_b200 import timing
+    s = cases.script("sram", 16, (8,), timing_seed=9)
+    s.enable_timing_arrivals()
+    cycles, window = 30, 8
+    states = cases.stimulus("sram", s, cycles)
+    cons = cases.constraint_buffer("sram", s, clock_ps=120, setup=30, hold=150)
+    eff = states.shape[1]
+    # oracle, window by window
+    st = states.reshape(-1).copy()
+    sram = np.zeros(max(1, s.sram_storage_size), np.uint32)
+    sram_x = np.full_like(sram, 0xFFFFFFFF)
+    want_stats = timing.new_stats()
+    want_ev = []
+    for c0 in range(0, cycles, window):
+        n = min(window, cycles - c0)
+        view = st[c0 * eff:]
+        ev, cnt = oracle_lib.simulate(s, view, n, eff, sram=sram, sram_x=sram_x, constraints=cons,
+                                      event_cap=1 << 16, arrival_state_offset=s.arrival_state_offset)
+        rec = ev.view(np.uint32).reshape(-1, 8).copy()
+        rec[:, 2] += c0
+        want_ev.append(rec)
+        timing.process_events(rec, cnt, 1 << 16, want_stats)
+    # GPU
+    ds = sim.DeviceScript(s)
+    dst = sim.u32_to_dev(states.reshape(-1))
+    gs = sim.u32_to_dev(np.zeros(max(1, s.sram_storage_size), np.uint32))
+    gsx = sim.u32_to_dev(np.full(max(1, s.sram_storage_size), 0xFFFFFFFF, np.uint32))
+    b = timing.ReportBuilder({"clock_period_ps": 120})
+    got_stats = timing.run_timed(ds, dst, cycles, eff, gs, gsx, sim.u32_to_dev(cons), window, 1 << 16,
+                                 s.arrival_state_offset, builder=b)
+    s.timing_arrivals_enabled = False
+    s.arrival_state_offset = 0
+    assert np.array_equal(sim.dev_to_u32(dst), st)
+    assert got_stats == want_stats and got_stats["setup_violations"] + got_stats["hold_violations"] > 0
+    rep = b.finalize(cycles, got_stats)
+    got_multiset = sorted((v["cycle"], v["kind"], v["word_id"], v["slack_ps"]) for v in rep["violations"])
+    want_multiset = sorted((int(r[2]), "setup" if r[0] == 4 else "hold", int(r[4]), timing._s32(r[5]))
+                           for r in np.concatenate(want_ev))
+    assert got_multiset == want_multiset
