@@ -63,6 +63,7 @@ void simulate_v1_noninteractive_timed_cuda(
 #define JQ_ERR_BARRIER_TIMEOUT -3 /* a grid barrier wait ran out */
 #define JQ_ERR_CUDA -4            /* asynchronous CUDA error */
 #define JQ_ERR_TOO_MANY_BLOCKS -5 /* grid larger than co-resident capacity */
+#define JQ_ERR_NOALLOC_LIMIT -6   /* request exceeds a fixed built-in workspace */
 #define JQ_ERR_EVENT_OVERFLOW 1   /* positive: events were dropped */
 
 /* Event record: identical to the reference's Event (32 bytes). */
@@ -199,6 +200,19 @@ size_t jq_mlp_scratch_floats(uint32_t ctas);
 /* One mini-batch: forward, backward of the mean squared error, gradient
  * reduction and (apply=1) an Adam step (beta1 0.9, beta2 0.999, eps 1e-8). */
 int jq_mlp_train_step(const jq_mlp_step_args *a);
+
+/* No counterpart in the reference.  Same as jq_mlp_train_step but allocates
+ * nothing and ignores a->scratch: the per-CTA gradient workspace is a
+ * file-scope device array of JQ_MLP_NOALLOC_MAX_CTAS rows (about 1.3 MB, held
+ * on every GPU that loads the library until exit).  For callers that cannot
+ * call cudaMalloc, e.g. while a CUDA graph is being captured or under a fixed
+ * pre-sized device pool.  a->scratch_ctas must be 1..JQ_MLP_NOALLOC_MAX_CTAS,
+ * otherwise JQ_ERR_NOALLOC_LIMIT.  The first call on a device resolves the
+ * array's address and should come before any stream capture.  All calls on
+ * a device share the array: calls that overlap on the GPU race.  Nothing in
+ * it needs clearing; each call writes every entry it reads. */
+#define JQ_MLP_NOALLOC_MAX_CTAS 16
+int jq_mlp_train_step_noalloc(const jq_mlp_step_args *a);
 
 /* Human-readable text for a status code. */
 const char *jq_strerror(int code);

@@ -393,6 +393,8 @@ const char *jq_strerror(int code) {
     case JQ_ERR_CUDA: return "CUDA error";
     case JQ_ERR_TOO_MANY_BLOCKS: return "more blocks than can be co-resident";
     case JQ_ERR_EVENT_OVERFLOW: return "event buffer overflowed";
+    case JQ_ERR_NOALLOC_LIMIT:
+      return "request exceeds the built-in no-allocation workspace (JQ_MLP_NOALLOC_MAX_CTAS CTAs)";
     default: return "unknown status";
   }
 }
