@@ -213,7 +213,7 @@ def run_mine_plain(args, rank, world):
     script_b, state_b = algorithmic_bytes_per_cycle(s)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=1, clocks=ck.summary(),
                 bytes_per_cycle=script_b + state_b, kernel_ms=dev_ms / args.steps,
-                h2d=host_pin.numel() * 4, d2h=out_pin.numel() * 4, launches_per_step=1,
+                h2d=host_pin.numel() * 4, d2h=out_pin.numel() * 4, launches_per_step=2,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=nb),
@@ -249,7 +249,7 @@ def run_mine_batched(args, rank, world):
     # snapshot 0: inputs of cycle 0, every DFF/SRAM word X
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
     snap0 = np.zeros((lanes, B.sig), np.uint32)
-    xt = state.xmask_template(s)
+    xt = state.xmask_all_state_x(s)
     rio = s.reg_io_state_size
     xt_b = batched.to_batched(np.repeat(xt[None, :], streams, axis=0))
     snap0[:, rio * 32:2 * rio * 32] = xt_b
@@ -293,7 +293,7 @@ def run_mine_batched(args, rank, world):
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams,
                 clocks=ck.summary(), bytes_per_cycle=script_b + state_b * streams,
                 kernel_ms=dev_ms / args.steps, h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4,
-                launches_per_step=1,
+                launches_per_step=2,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
@@ -354,7 +354,8 @@ def main():
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
     ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
-    ap.add_argument("--cpu-cycles", type=int, default=48)
+    ap.add_argument("--cpu-cycles", type=int, default=160,
+                    help="CPU baseline sample: cycles of one stream (about 10 s single-threaded)")
     ap.add_argument("--clusters", type=int, default=512,
                     help="design size in 4096-gate clusters (512 = the 2M-gate workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

@@ -73,6 +73,18 @@ def xmask_template(script):
     return t
 
 
+def xmask_all_state_x(script):
+    """X-mask words of an initial snapshot with every DFF and SRAM-read bit X:
+    only the input_layout pins (primary inputs, clock flags) are known.  The
+    reference CLI clears X on DFF-Q positions (the template above); a run that
+    starts from an unknown register state sets this mask in snapshot 0."""
+    rio = script.reg_io_state_size
+    t = np.full(rio, 0xFFFFFFFF, dtype=np.uint32)
+    for p in input_positions(script).tolist():
+        t[p >> 5] &= np.uint32(~(1 << (p & 31)) & 0xFFFFFFFF)
+    return t
+
+
 def expand_states_for_xprop(value_states, script):
     """[values | xmask template] per snapshot (src/sim/vcd_io.rs:465-484)."""
     rio = script.reg_io_state_size

@@ -55,9 +55,13 @@ def stimulus(kind, s, cycles, seed=3, p_toggle=0.5, reset_cycles=2, x_init=False
 
 def constraint_buffer(kind, s, clock_ps=10_000, setup=30, hold=10, seed=5):
     """[clock, per-word setup<<16|hold] with per-DFF clock arrival U[0,300]."""
+    return constraint_buffer_for(design(kind), s, clock_ps, setup, hold, seed)
+
+
+def constraint_buffer_for(d, s, clock_ps=10_000, setup=30, hold=10, seed=5):
+    """Same, for a design object: jqf_constraint_buffer over every DFF."""
     import ctypes
-    from jacquard_b200._native import load
-    d = design(kind)
+    from jacquard_b200.frontend import _lib
     rng = np.random.default_rng(seed)
     n = int(d.num_dffs)
     su = np.full(n, setup, np.uint16)
@@ -66,11 +70,9 @@ def constraint_buffer(kind, s, clock_ps=10_000, setup=30, hold=10, seed=5):
     pos = np.ascontiguousarray(s.dff_data_pos, dtype=np.uint32)
     out = np.zeros(s.reg_io_state_size, np.uint32)
     clk = ctypes.c_uint32()
-    from jacquard_b200.frontend import _lib
-    L = _lib()
-    L.jqf_constraint_buffer(ctypes.c_uint32(s.reg_io_state_size), ctypes.c_uint64(clock_ps),
-                            ctypes.c_size_t(n), su.ctypes.data_as(ctypes.c_void_p),
-                            ho.ctypes.data_as(ctypes.c_void_p), ca.ctypes.data_as(ctypes.c_void_p),
-                            pos.ctypes.data_as(ctypes.c_void_p), ctypes.byref(clk),
-                            out.ctypes.data_as(ctypes.c_void_p))
+    _lib().jqf_constraint_buffer(ctypes.c_uint32(s.reg_io_state_size), ctypes.c_uint64(clock_ps),
+                                 ctypes.c_size_t(n), su.ctypes.data_as(ctypes.c_void_p),
+                                 ho.ctypes.data_as(ctypes.c_void_p), ca.ctypes.data_as(ctypes.c_void_p),
+                                 pos.ctypes.data_as(ctypes.c_void_p), ctypes.byref(clk),
+                                 out.ctypes.data_as(ctypes.c_void_p))
     return np.concatenate([[np.uint32(clk.value)], out]).astype(np.uint32)
