@@ -44,28 +44,64 @@ def peaks():
 
 
 class Clocks:
-    """Samples SM clocks and throttle reasons while the timed region runs."""
+    """Samples SM clocks and throttle reasons while the timed region runs
+    (NVML, read-only queries, every 20 ms; nvidia-smi when NVML is absent)."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu=0):
         self.gpu = gpu
-        self.rows = []
+        self.sm, self.sm_max, self.reasons = [], [], set()
         self._stop = threading.Event()
         self._t = None
 
-    def _loop(self):
+    def _nvml_loop(self, nv):
+        h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+        masks = [(n, getattr(nv, c)) for n, c in self.REASONS]
+        while not self._stop.is_set():
+            self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+            self.sm_max.append(float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)))
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            for n, m in masks:
+                if r & m:
+                    self.reasons.add(n)
+            self._stop.wait(0.02)
+
+    def _smi_loop(self):
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                                       "--format=csv,noheader,nounits"], capture_output=True,
                                      text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
+                r = [x.strip() for x in out.split(",")]
+                if len(r) >= 9:
+                    if r[1].replace(".", "").isdigit():
+                        self.sm.append(float(r[1]))
+                    if r[2].replace(".", "").isdigit():
+                        self.sm_max.append(float(r[2]))
+                    for i, (n, _) in enumerate(self.REASONS):
+                        if r[5 + i].lower() == "active":
+                            self.reasons.add(n)
             except Exception:
                 pass
             self._stop.wait(0.2)
+
+    def _loop(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+        except Exception:
+            self._smi_loop()
+            return
+        try:
+            self._nvml_loop(nv)
+        finally:
+            nv.nvmlShutdown()
 
     def __enter__(self):
         self._t = threading.Thread(target=self._loop, daemon=True)
@@ -77,19 +113,11 @@ class Clocks:
         self._t.join(timeout=10)
 
     def summary(self):
-        if not self.rows:
+        if not self.sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.rows)}
+        return {"sm_mhz": float(np.median(self.sm)),
+                "sm_max_mhz": max(self.sm_max) if self.sm_max else None,
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
 def build_design(seed=2, clusters=512, n_dff=200_000):
@@ -347,7 +375,7 @@ def cpu_baseline(s, d, cycles=8, threads=1):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--mode", default="batched", choices=["plain", "batched"])

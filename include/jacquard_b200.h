@@ -120,7 +120,8 @@ int jq_max_blocks(int device, size_t *max_blocks);
 typedef struct {
   size_t num_blocks, num_major_stages;
   const size_t *blocks_start;  /* device */
-  const uint32_t *blocks_data; /* device, 16-byte aligned */
+  const uint32_t *blocks_data; /* device, 16-byte aligned, prepared by
+                                  jq_batched_prepare */
   uint32_t lanes;              /* lane words (32 streams each) */
   uint32_t *sram_data, *sram_xmask; /* device: [stream][sram_words_per_stream] */
   size_t sram_words_per_stream;
@@ -154,6 +155,13 @@ typedef struct {
   void *stream;
 } jq_batch_args;
 
+/* Rewrites a script (FlattenedScriptV1 blocks_data, device) into `out`
+ * (device, blocks_data_len words, 16-byte aligned) in the batched
+ * interpreter's layout: same size and partition offsets, boomerang chunks
+ * reordered per thread.  Asynchronous on `stream`.  Run once per script. */
+int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
+                       size_t blocks_data_len, size_t num_blocks, size_t num_major_stages,
+                       uint32_t *out, void *stream);
 int jq_simulate_batched(const jq_batch_args *a);
 /* Synchronizes `stream`; JQ_OK or the kernel's recorded error. */
 int jq_batched_status(void *stream);

@@ -39,6 +39,9 @@ def lib():
         L.jq_batched_status.argtypes = [vp]
         L.jq_batched_max_blocks.restype = ctypes.c_int
         L.jq_batched_max_blocks.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_size_t)]
+        L.jq_batched_prepare.restype = ctypes.c_int
+        L.jq_batched_prepare.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+                                         vp, vp]
         L._jq_batched_typed = True
     return L
 
@@ -117,11 +120,20 @@ def block_lists(script):
 class BatchedSim:
     """Script + buffers on the device for `lanes` lane words (32*lanes streams)."""
 
-    def __init__(self, script, lanes, device="cuda", record=False, po_signals=None, grid=0):
+    def __init__(self, script, lanes, device="cuda", record=False, po_signals=None, grid=0,
+                 wo_slots=None):
         self.script = script
         self.lanes = lanes
         self.device = torch.device(device)
         self.ds = sim.DeviceScript(script, self.device)
+        # the kernel reads the script in its own prepared layout
+        self.prepared = torch.empty_like(self.ds.blocks_data)
+        rc = lib().jq_batched_prepare(self.ds.blocks_start.data_ptr(), self.ds.blocks_data.data_ptr(),
+                                      self.ds.blocks_data.numel(), self.ds.num_blocks,
+                                      self.ds.num_major_stages, self.prepared.data_ptr(),
+                                      torch.cuda.current_stream(self.device).cuda_stream)
+        if rc:
+            raise RuntimeError("jq_batched_prepare: " + sim.lib().jq_strerror(rc).decode())
         self.eff = getattr(script, "effective_words", None) or \
             script.reg_io_state_size * (2 if script.xprop_enabled else 1)
         self.sig = self.eff * 32
@@ -133,7 +145,9 @@ class BatchedSim:
             r = np.asarray(regions, np.uint32).reshape(-1, 3)
             self.in_sigs = int(r[:, 2].sum())
             self.regions = torch.from_numpy(r.reshape(-1).view(np.int32)).to(self.device)
-        self.wo_slots = max(1, max_num_ios(script))
+        # writeout capacity: the largest num_ios, or more (256 selects the
+        # single-buffered tree state, whose shared memory fits any script)
+        self.wo_slots = max(1, max_num_ios(script)) if wo_slots is None else wo_slots
         bl, bls = block_lists(script)
         self.block_list = torch.from_numpy(bl.view(np.int32)).to(self.device)
         self.block_list_start = torch.from_numpy(bls.view(np.int32)).to(self.device)
@@ -178,7 +192,7 @@ class BatchedSim:
         L = lib()
         wave_ptr = wave.data_ptr() if wave is not None else None
         a = BatchArgs(self.ds.num_blocks, self.ds.num_major_stages, self.ds.blocks_start.data_ptr(),
-                      self.ds.blocks_data.data_ptr(), self.lanes, self.sram.data_ptr(),
+                      self.prepared.data_ptr(), self.lanes, self.sram.data_ptr(),
                       self.sram_x.data_ptr(), self.sram_words, cycles, self.sig,
                       self.state_a.data_ptr(), self.state_b.data_ptr(),
                       stim.data_ptr() if stim is not None else None, self.in_sigs,

@@ -93,20 +93,40 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64
   }
 }
 
-// 16-bit shuffle index q (0..8191) of a 5120-word chunk: the plain layout
-// puts bit k of thread T at chunk[(k>>3)*1024 + T*4 + ((k>>1)&3)], low half
-// for even k.
-__device__ __forceinline__ uint32_t perm_at(const uint32_t *chunk, uint32_t q) {
+// 16-bit shuffle index q (0..8191) of a chunk in the script's own layout:
+// bit k of thread T at chunk[(k>>3)*1024 + T*4 + ((k>>1)&3)], low half for
+// even k (src/flatten.rs:984-1076).
+__device__ __forceinline__ uint32_t perm_src(const uint32_t *chunk, uint32_t q) {
   const uint32_t T = q >> 5, k = q & 31;
   const uint32_t w = chunk[(k >> 3) * 1024 + T * 4 + ((k >> 1) & 3)];
   return (k & 1) ? (w >> 16) : (w & 0xffffu);
 }
+// Shuffle index q of a prepared SRAM/duplicate or clock-enable chunk:
+// entries in q order, two per word.
+__device__ __forceinline__ uint32_t perm_lin(const uint32_t *chunk, uint32_t q) {
+  const uint32_t w = chunk[q >> 1];
+  return (q & 1) ? (w >> 16) : (w & 0xffffu);
+}
 // Tree-state address of position p in shared memory: a bijective XOR
 // swizzle that gives the 32 lanes of a warp distinct banks under the
 // residue ownership map (lane bits sit at position bits 4..8).
-__device__ __forceinline__ uint32_t sw(uint32_t p) { return p ^ ((p >> 4) & 31u); }
+__host__ __device__ __forceinline__ uint32_t sw(uint32_t p) { return p ^ ((p >> 4) & 31u); }
 __device__ __forceinline__ uint32_t bitmask(uint32_t word, uint32_t q) {
   return 0u - ((word >> (q & 31)) & 1u);
+}
+// All-ones when bit `i` (a compile-time constant) of w is set.
+template <int i>
+__device__ __forceinline__ uint32_t mk(uint32_t w) {
+  return (uint32_t)((int32_t)(w << (31 - i)) >> 31);
+}
+// Residue of thread t under the tree ownership map: warp w, lane l -> w | l<<4.
+__host__ __device__ __forceinline__ uint32_t residue(uint32_t t) { return (t >> 5) | ((t & 31u) << 4); }
+// Tree position i (0..15) of the thread with residue u: level-1..4 positions
+// u + 512k, then u itself (levels 5..9, when u >= 16).
+__host__ __device__ __forceinline__ uint32_t owned_pos(uint32_t u, int i) {
+  return i < 8 ? 4096 + u + 512 * i
+               : i < 12 ? 2048 + u + 512 * (i - 8)
+                        : i < 14 ? 1024 + u + 512 * (i - 12) : i == 14 ? 512 + u : u;
 }
 
 struct Shared {
@@ -117,14 +137,28 @@ struct Shared {
 };
 
 // One (block, lane) work item: the block's partition list for one lane word.
-// Tree state S and writeouts WO hold (value, X) pairs so one shared-memory
-// access moves both lanes; flags are read as one uint4 (xa, xb, ob, delay).
+// Tree state and writeouts hold (value, X) pairs so one shared-memory access
+// moves both.  The script is in the prepared layout (jq_batched_prepare):
+//   boomerang chunk: words [0, 4096) two uint4 planes [2][512 threads], the
+//     thread's 16 gather sources (level-1 inputs a then b, already swizzled);
+//     words [4096, 5120) one uint2 per thread: xa bits 0..15 | xb bits 16..31,
+//     ob bits 0..15 of its 16 owned positions, and for warp-0 threads t < 8
+//     the flags of tree positions 8+t, 4+t, 2+t, 1+t (levels 10..13) at
+//     bits 16+m (xa), 20+m (xb), 24+m (ob) of the second word;
+//   SRAM/duplicate and clock-enable chunks: shuffle entries in q order,
+//     flags unchanged.
+// With `ds` the tree state is double-buffered (stage ci reads buffer ci&1 and
+// writes the other), which removes the barrier between gather and overwrite.
+template <bool DS>
 __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, uint32_t *chunks,
                          uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                          const uint32_t *in, uint32_t *out, uint32_t lane, uint32_t pid0,
                          bool &failed) {
   const int t = threadIdx.x;
   const size_t lane_base = (size_t)lane * P.sig_per_snap;
+  constexpr bool ds = DS;
+  uint2 *const Sb0 = S;
+  uint2 *const Sb1 = ds ? S + 8192 : S;
   size_t off = 0;
   uint32_t pid = pid0;
   for (;;) {
@@ -149,14 +183,14 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
       tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
     }
 
-    // ---- global read, in two phases so that the loads overlap (hooks of the
-    // previous partition read S before this point: the loop-top barrier):
+    // ---- global read into tree buffer 0, in two phases so that the loads
+    // overlap:
     // (a) thread t < 256 enumerates its (idx, mask) bits and stores, at the
     //     destination position, the source signal (bit 31 = current-cycle
     //     staged IO) or NONE for the unfilled tail; positions follow the
     //     kernel's append order (first appended bit ends up most significant);
     // (b) all threads load their 16 positions with independent loads.
-    uint32_t *Sv = reinterpret_cast<uint32_t *>(S);  // staging: .x words
+    uint32_t *Sv = reinterpret_cast<uint32_t *>(Sb0);  // staging: .x words
     if (t < 256) {
       uint2 pr[16];
 #pragma unroll
@@ -210,177 +244,169 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         }
       }
 #pragma unroll
-      for (int k = 0; k < 16; ++k) S[sw(t + BT * k)] = make_uint2(v[k], vx[k]);
+      for (int k = 0; k < 16; ++k) Sb0[sw(t + BT * k)] = make_uint2(v[k], vx[k]);
     }
 
     // Thread -> tree residue map: thread (warp w, lane l) owns positions whose
     // value mod 512 is u = w | l << 4.  Levels 1..4 then read only the
     // thread's own registers, levels 5..9 read lanes of the same warp
     // (residue bits 4..8 are lane bits), and only positions 1..15 need one
-    // exchange through shared memory.
+    // exchange through shared memory.  Under the swizzle every owned
+    // position p = base + u has address base + us.
     const uint32_t lane_i = t & 31, warp_i = t >> 5;
-    const uint32_t u = warp_i | (lane_i << 4);
+    const uint32_t u = residue(t);
+    const uint32_t us = sw(u);
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
       const uint32_t b = ci & 1;
       uint32_t *C = chunks + b * STAGE_WORDS;
+      if (ci == 0) __syncthreads();  // global read complete
       // The other buffer's last reader finished before the final barrier of
       // the previous chunk, so the next chunk can be issued right away.
-      if (ci == 0) __syncthreads();
       if (t == 0 && ci + 1 < nchunks) {
         mbar_expect_tx(&sh.bar[b ^ 1], CHUNK_BYTES);
         tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * (ci + 1),
                     CHUNK_BYTES, &sh.bar[b ^ 1]);
       }
       uint32_t &uses = b ? uses1 : uses0;
-      if (!mbar_wait(&sh.bar[b], uses & 1u, P.timeout)) {
-        failed = true;
-        // let any copy still in flight into this CTA land before leaving
-        if (t == 0) {
-          mbar_wait(&sh.bar[0], uses0 & 1u, P.timeout);
-          mbar_wait(&sh.bar[1], uses1 & 1u, P.timeout);
-        }
-      }
+      // warp-uniform, so the shuffles below run with full warps
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.timeout));
       ++uses;
-      if (__syncthreads_or(failed)) {
-        failed = true;
-        return;
-      }
-      const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);  // xa, xb, ob, pad
-#define JQ_FL(p, XA, XB, OB)                    \
-  const uint4 fl_##XA = F4[(p) >> 5];           \
-  const uint32_t XA = bitmask(fl_##XA.x, (p));  \
-  const uint32_t XB = bitmask(fl_##XA.y, (p));  \
-  const uint32_t OB = bitmask(fl_##XA.z, (p));
-
+      // a chunk never arrived: every thread leaves together, after letting
+      // the copy still in flight into the other buffer land
+#define JQ_FAIL_IF(cond)                                               \
+  if (__syncthreads_or(cond)) {                                        \
+    failed = true;                                                     \
+    if (t == 0) mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.timeout); \
+    return;                                                            \
+  }
       if (ci < ns) {
         // ---------------- boomerang stage ci
-        // level 1 (positions 4096 + j): gather both inputs into registers
+        const uint2 *Sp = (ci & 1) ? Sb1 : Sb0;
+        uint2 *Sn = (ci & 1) ? Sb0 : Sb1;
         uint2 ga[8], gb[8];
+        uint32_t A = 0, B = 0;
+        if (ok) {
+          const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
+          const uint4 pa = P4[t], pb = P4[BT + t];
+          const uint2 fl = reinterpret_cast<const uint2 *>(C + 4096)[t];
+          A = fl.x;
+          B = fl.y;
+          ga[0] = Sp[pa.x & 0xffffu]; ga[1] = Sp[pa.x >> 16];
+          ga[2] = Sp[pa.y & 0xffffu]; ga[3] = Sp[pa.y >> 16];
+          ga[4] = Sp[pa.z & 0xffffu]; ga[5] = Sp[pa.z >> 16];
+          ga[6] = Sp[pa.w & 0xffffu]; ga[7] = Sp[pa.w >> 16];
+          gb[0] = Sp[pb.x & 0xffffu]; gb[1] = Sp[pb.x >> 16];
+          gb[2] = Sp[pb.y & 0xffffu]; gb[3] = Sp[pb.y >> 16];
+          gb[4] = Sp[pb.z & 0xffffu]; gb[5] = Sp[pb.z >> 16];
+          gb[6] = Sp[pb.w & 0xffffu]; gb[7] = Sp[pb.w >> 16];
+        }
+        if (!ds) {
+          // single buffer: all gathers done before the in-place overwrite
+          JQ_FAIL_IF(!ok)
+        }
+        if (ok) {
+          // level 1 (positions 4096 + u + 512k)
+          uint32_t v1[8], x1[8];
+#define JQ_L1(k)                                                                         \
+  xand(ga[k].x, ga[k].y, gb[k].x, gb[k].y, mk<k>(A), mk<16 + k>(A), mk<k>(B), v1[k], x1[k]); \
+  Sn[4096 + 512 * k + us] = make_uint2(v1[k], x1[k]);
+          JQ_L1(0) JQ_L1(1) JQ_L1(2) JQ_L1(3) JQ_L1(4) JQ_L1(5) JQ_L1(6) JQ_L1(7)
+#undef JQ_L1
+          uint32_t v2[4], x2[4];
+#define JQ_L2(k)                                                                           \
+  xand(v1[k], x1[k], v1[k + 4], x1[k + 4], mk<8 + k>(A), mk<24 + k>(A), mk<8 + k>(B), v2[k], \
+       x2[k]);                                                                             \
+  Sn[2048 + 512 * k + us] = make_uint2(v2[k], x2[k]);
+          JQ_L2(0) JQ_L2(1) JQ_L2(2) JQ_L2(3)
+#undef JQ_L2
+          uint32_t v3[2], x3[2];
+          xand(v2[0], x2[0], v2[2], x2[2], mk<12>(A), mk<28>(A), mk<12>(B), v3[0], x3[0]);
+          Sn[1024 + us] = make_uint2(v3[0], x3[0]);
+          xand(v2[1], x2[1], v2[3], x2[3], mk<13>(A), mk<29>(A), mk<13>(B), v3[1], x3[1]);
+          Sn[1536 + us] = make_uint2(v3[1], x3[1]);
+          uint32_t v4, x4;
+          xand(v3[0], x3[0], v3[1], x3[1], mk<14>(A), mk<30>(A), mk<14>(B), v4, x4);
+          Sn[512 + us] = make_uint2(v4, x4);
+          // levels 5..9: the thread's position u (u >= 16) at the level of
+          // its lane: level 5 (lanes 16..31) from level-4 residues u-256
+          // (lane ^ 16) and u; level 6+k' (lanes [2^k, 2^(k+1))) from lanes
+          // l + 2^k and l + 2^(k+1)
+          const uint32_t XA = mk<15>(A), XB = mk<31>(A), OB = mk<15>(B);
+          uint32_t cv, cx;
+          {
+            const uint32_t a = __shfl_xor_sync(0xffffffffu, v4, 16);
+            const uint32_t ax = __shfl_xor_sync(0xffffffffu, x4, 16);
+            xand(a, ax, v4, x4, XA, XB, OB, cv, cx);
+            if (lane_i >= 16) Sn[us] = make_uint2(cv, cx);
+          }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const uint32_t j = u + 512 * k;
-          ga[k] = S[sw(perm_at(C, j))];
-          gb[k] = S[sw(perm_at(C, j + 4096))];
-        }
-        __syncthreads();  // all gathers done before the in-place overwrite
-        uint32_t v1[8], x1[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const uint32_t p = 4096 + u + 512 * k;
-          JQ_FL(p, XA, XB, OB)
-          xand(ga[k].x, ga[k].y, gb[k].x, gb[k].y, XA, XB, OB, v1[k], x1[k]);
-          if (!is_x) x1[k] = 0;
-          S[sw(p)] = make_uint2(v1[k], x1[k]);
-        }
-        uint32_t v2[4], x2[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const uint32_t p = 2048 + u + 512 * k;
-          JQ_FL(p, XA, XB, OB)
-          xand(v1[k], x1[k], v1[k + 4], x1[k + 4], XA, XB, OB, v2[k], x2[k]);
-          if (!is_x) x2[k] = 0;
-          S[sw(p)] = make_uint2(v2[k], x2[k]);
-        }
-        uint32_t v3[2], x3[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const uint32_t p = 1024 + u + 512 * k;
-          JQ_FL(p, XA, XB, OB)
-          xand(v2[k], x2[k], v2[k + 2], x2[k + 2], XA, XB, OB, v3[k], x3[k]);
-          if (!is_x) x3[k] = 0;
-          S[sw(p)] = make_uint2(v3[k], x3[k]);
-        }
-        uint32_t v4, x4;
-        {
-          const uint32_t p = 512 + u;
-          JQ_FL(p, XA, XB, OB)
-          xand(v3[0], x3[0], v3[1], x3[1], XA, XB, OB, v4, x4);
-          if (!is_x) x4 = 0;
-          S[sw(p)] = make_uint2(v4, x4);
-        }
-        // level 5: position u (lanes 16..31) from level-4 u-256 (lane ^ 16) and u
-        uint32_t cv, cx;
-        {
-          const uint32_t a = __shfl_xor_sync(0xffffffffu, v4, 16);
-          const uint32_t ax = __shfl_xor_sync(0xffffffffu, x4, 16);
-          const uint32_t p = u;
-          JQ_FL(p & 511, XA, XB, OB)
-          xand(a, ax, v4, x4, XA, XB, OB, cv, cx);
-          if (!is_x) cx = 0;
-          if (lane_i >= 16) S[sw(p)] = make_uint2(cv, cx);
-        }
-        // levels 6..9: the parent of residue u with lane bit k set (lanes
-        // [2^k, 2^(k+1))) reads lanes l + 2^k and l + 2^(k+1)
-#pragma unroll
-        for (int k = 3; k >= 0; --k) {
-          const uint32_t d = 1u << k;
-          const uint32_t a = __shfl_sync(0xffffffffu, cv, (lane_i + d) & 31);
-          const uint32_t bb = __shfl_sync(0xffffffffu, cv, (lane_i + 2 * d) & 31);
-          const uint32_t ax = __shfl_sync(0xffffffffu, cx, (lane_i + d) & 31);
-          const uint32_t bx = __shfl_sync(0xffffffffu, cx, (lane_i + 2 * d) & 31);
-          if (lane_i >= d && lane_i < 2 * d) {
-            const uint32_t p = u;
-            JQ_FL(p, XA, XB, OB)
-            xand(a, ax, bb, bx, XA, XB, OB, cv, cx);
-            if (!is_x) cx = 0;
-            S[sw(p)] = make_uint2(cv, cx);
+          for (int k = 3; k >= 0; --k) {
+            const uint32_t d = 1u << k;
+            const uint32_t a = __shfl_sync(0xffffffffu, cv, (lane_i + d) & 31);
+            const uint32_t bb = __shfl_sync(0xffffffffu, cv, (lane_i + 2 * d) & 31);
+            const uint32_t ax = __shfl_sync(0xffffffffu, cx, (lane_i + d) & 31);
+            const uint32_t bx = __shfl_sync(0xffffffffu, cx, (lane_i + 2 * d) & 31);
+            if (lane_i >= d && lane_i < 2 * d) {
+              xand(a, ax, bb, bx, XA, XB, OB, cv, cx);
+              Sn[us] = make_uint2(cv, cx);
+            }
           }
         }
-        __syncthreads();
+        JQ_FAIL_IF(!ok)
         // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
         if (t < 32) {
-          uint2 h = t < 16 ? S[sw(16 + t)] : make_uint2(0, 0);
+          uint2 h = t < 16 ? Sn[sw(16 + t)] : make_uint2(0, 0);
           uint32_t hv = h.x, hx = h.y;
 #pragma unroll
-          for (uint32_t len = 8; len >= 1; len >>= 1) {
+          for (int m = 0; m < 4; ++m) {
+            const uint32_t len = 8u >> m;
             const uint32_t bb = __shfl_sync(0xffffffffu, hv, (t + len) & 31);
             const uint32_t bx = __shfl_sync(0xffffffffu, hx, (t + len) & 31);
             if ((uint32_t)t < len) {
-              const uint32_t p = len + t;
-              JQ_FL(p, XA, XB, OB)
               uint32_t r, rx;
-              xand(hv, hx, bb, bx, XA, XB, OB, r, rx);
-              if (!is_x) rx = 0;
-              S[sw(p)] = make_uint2(r, rx);
+              xand(hv, hx, bb, bx, 0u - ((B >> (16 + m)) & 1u), 0u - ((B >> (20 + m)) & 1u),
+                   0u - ((B >> (24 + m)) & 1u), r, rx);
+              Sn[len + t] = make_uint2(r, rx);
               hv = r;
               hx = rx;
             }
           }
-          if (t == 0) S[0] = make_uint2(0, 0);
+          if (t == 0) Sn[0] = make_uint2(0, 0);
         }
         __syncthreads();
-        // writeout hooks of this stage
-        for (uint32_t q = t; q < num_ios * 32; q += BT) {
-          const uint32_t slot = q >> 5;
+        // writeout hooks of this stage: warp w scans slots w, w+16, ...
+        for (uint32_t slot = warp_i; slot < num_ios; slot += BT / 32) {
           const uint32_t hw = sh.meta[128 + slot / 2];
           const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
-          if ((hook >> 8) == ci) WO[q] = S[sw((hook & 255u) * 32 + (q & 31))];
+          if ((hook >> 8) == ci) WO[slot * 32 + lane_i] = Sn[sw((hook & 255u) * 32 + lane_i)];
         }
       } else if (ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports
+        JQ_FAIL_IF(!ok)  // hooks done, chunk landed
+        uint2 *St = Sb0;  // staging (the last stage's hooks are done)
+        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
-        // stage the permuted words in S (free now: all hooks are done)
         for (uint32_t q = t; q < nq; q += BT) {
-          const uint2 w = WO[perm_at(C, q)];
+          const uint2 w = WO[perm_lin(C, q)];
           const uint4 fl = F4[q >> 5];
           const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q);
-          S[q] = make_uint2((w.x & ~set0) ^ inv, is_x ? (w.y & ~set0) : 0u);
+          St[q] = make_uint2((w.x & ~set0) ^ inv, is_x ? (w.y & ~set0) : 0u);
         }
         __syncthreads();
         // one warp per SRAM, lane = stream within the lane word
         const int warp = t >> 5, ln = t & 31;
         for (uint32_t i = warp; i < num_srams; i += BT / 32) {
-          const uint2 *A = S + (4 * i) * 32;
+          const uint2 *Aw = St + (4 * i) * 32;
           uint32_t ra = 0, wa = 0, en = 0, data = 0, datax = 0;
 #pragma unroll
           for (int k = 0; k < 16; ++k) {
-            ra |= ((A[k].x >> ln) & 1u) << k;
-            wa |= ((A[16 + k].x >> ln) & 1u) << k;
+            ra |= ((Aw[k].x >> ln) & 1u) << k;
+            wa |= ((Aw[16 + k].x >> ln) & 1u) << k;
           }
 #pragma unroll 8
           for (int k = 0; k < 32; ++k) {
-            en |= ((A[32 + k].x >> ln) & 1u) << k;
-            const uint2 dk = A[64 + k];
+            en |= ((Aw[32 + k].x >> ln) & 1u) << k;
+            const uint2 dk = Aw[64 + k];
             data |= ((dk.x >> ln) & 1u) << k;
             datax |= ((dk.y >> ln) & 1u) << k;
           }
@@ -408,11 +434,13 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           }
         }
         for (uint32_t q = t; q < num_dup * 32; q += BT)
-          WO[(num_ios - num_srams - num_dup) * 32 + q] = S[num_srams * 4 * 32 + q];
+          WO[(num_ios - num_srams - num_dup) * 32 + q] = St[num_srams * 4 * 32 + q];
         __syncthreads();
       } else {
         // ---------------- clock-enable permutation and commit (4 words per
         // thread in flight)
+        JQ_FAIL_IF(!ok)
+        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
         for (uint32_t q0 = t; q0 < nq; q0 += 4 * BT) {
           uint32_t cp[4], cpx[4], wv[4], wx[4], old[4], oldx[4];
@@ -421,7 +449,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           for (int uu = 0; uu < 4; ++uu) {
             const uint32_t q = q0 + uu * BT;
             if (q < nq) {
-              const uint2 src = WO[perm_at(C, q)];
+              const uint2 src = WO[perm_lin(C, q)];
               const uint4 fl = F4[q >> 5];
               const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q),
                              dinv = bitmask(fl.z, q);
@@ -447,7 +475,6 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           }
         }
       }
-#undef JQ_FL
     }
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
     if (P.part_cycles) {
@@ -460,13 +487,15 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     if (is_last) break;
   }
 }
+#undef JQ_FAIL_IF
 
+template <bool DS>
 __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   extern __shared__ __align__(128) uint8_t dyn[];
   __shared__ Shared sh;
   uint32_t *chunks = reinterpret_cast<uint32_t *>(dyn);               // 2 x 20 KB
-  uint2 *S = reinterpret_cast<uint2 *>(chunks + 2 * STAGE_WORDS);      // 8192 (v, x)
-  uint2 *WO = S + 8192;                                               // wo_slots*32
+  uint2 *S = reinterpret_cast<uint2 *>(chunks + 2 * STAGE_WORDS);      // (1 or 2) x 8192 (v, x)
+  uint2 *WO = S + (DS ? 2 * 8192 : 8192);                             // wo_slots*32
   const int t = threadIdx.x;
   if (t == 0) {
     mbar_init(&sh.bar[0], 1);
@@ -516,7 +545,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
         const uint32_t *script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
         const uint32_t pid0 = P.part_base ? P.part_base[(size_t)ms * P.num_blocks + blk] : 0u;
-        run_item(P, sh, S, WO, chunks, uses0, uses1, script, in, out, lane, pid0, failed);
+        run_item<DS>(P, sh, S, WO, chunks, uses0, uses1, script, in, out, lane, pid0, failed);
         if (failed) {
           if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
           return;
@@ -567,6 +596,79 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   }
 }
 
+// Script preparation for this kernel (run once per script, on the device):
+// every boomerang chunk is rewritten thread-major -- the 16 gather sources of
+// each thread (swizzled tree addresses) as two uint4 planes and its owned
+// positions' flag bits as one uint2 -- and the SRAM/duplicate and
+// clock-enable chunks get their shuffle entries in q order.  Metadata, global
+// read sections and sizes are unchanged, so blocks_start stays valid.  One
+// CTA per (major stage, block) entry walks its partition list.
+__global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(const size_t *blocks_start,
+                                                                const uint32_t *src,
+                                                                uint32_t *dst, unsigned entries) {
+  const unsigned e = blockIdx.x;
+  if (e >= entries) return;
+  const uint32_t t = threadIdx.x;
+  const uint32_t u = residue(t);
+  size_t off = blocks_start[e];
+  for (;;) {
+    const uint32_t ns = src[off];
+    if (!ns) break;
+    const uint32_t is_last = src[off + 1], R = src[off + 6];
+    const uint32_t *ch = src + off + 256 + 512 * (size_t)R;
+    uint32_t *dch = dst + off + 256 + 512 * (size_t)R;
+    for (uint32_t ci = 0; ci < ns + 2; ++ci) {
+      const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
+      uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
+      if (ci < ns) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          // plane m>>2, word m&3: entries 8*(m>>2) + 2*(m&3) + {0, 1}; entry
+          // k < 8 is input a of position 4096+u+512k (source q = u+512k),
+          // entry 8+k its input b (q + 4096)
+          uint32_t w = 0;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t en = 8 * (m >> 2) + 2 * (m & 3) + h;
+            const uint32_t q = (en < 8) ? u + 512 * en : u + 512 * (en - 8) + 4096;
+            w |= sw(perm_src(C, q)) << (16 * h);
+          }
+          D[4 * ((m >> 2) * BT + t) + (m & 3)] = w;
+        }
+        uint32_t A = 0, B = 0;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const uint32_t p = owned_pos(u, i);
+          if (i == 15 && u < 16) continue;
+          const uint32_t *F = C + 4096 + 4 * (p >> 5);
+          A |= ((F[0] >> (p & 31)) & 1u) << i;
+          A |= ((F[1] >> (p & 31)) & 1u) << (16 + i);
+          B |= ((F[2] >> (p & 31)) & 1u) << i;
+        }
+        if (t < 8) {
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const uint32_t len = 8u >> m;
+            if (t >= len) continue;
+            const uint32_t p = len + t;
+            const uint32_t *F = C + 4096 + 4 * (p >> 5);
+            B |= ((F[0] >> (p & 31)) & 1u) << (16 + m);
+            B |= ((F[1] >> (p & 31)) & 1u) << (20 + m);
+            B |= ((F[2] >> (p & 31)) & 1u) << (24 + m);
+          }
+        }
+        D[4096 + 2 * t] = A;
+        D[4096 + 2 * t + 1] = B;
+      } else {
+        for (uint32_t q2 = t; q2 < 4096; q2 += BT)
+          D[q2] = perm_src(C, 2 * q2) | (perm_src(C, 2 * q2 + 1) << 16);
+      }
+    }
+    off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    if (is_last) break;
+  }
+}
+
 }  // namespace jqk
 
 using namespace jqk;
@@ -581,21 +683,53 @@ __global__ void jq_batched_reset_kernel(int slot) {
 
 extern "C" {
 
+static size_t smem_layout_bytes(uint32_t wo_slots, bool ds) {
+  return 2 * (size_t)CHUNK_BYTES + (ds ? 2 : 1) * 8192 * 8 + (size_t)wo_slots * 32 * 8;
+}
+
+// Double-buffered tree state when it fits next to the writeouts.
+static bool use_double_buffer(uint32_t wo_slots) {
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, jq_batched_kernel<true>) != cudaSuccess)
+    return false;
+  return smem_layout_bytes(wo_slots, true) + fa.sharedSizeBytes <= (size_t)optin;
+}
+
 int jq_batched_smem_bytes(uint32_t wo_slots) {
-  return (int)(2 * CHUNK_BYTES + 2 * 8192 * 4 + 2 * wo_slots * 32 * 4);
+  return (int)smem_layout_bytes(wo_slots, use_double_buffer(wo_slots));
 }
 
 int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
-  int smem = jq_batched_smem_bytes(wo_slots);
-  if (cudaFuncSetAttribute(jq_batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-      cudaSuccess)
+  const bool ds = use_double_buffer(wo_slots);
+  const void *fn = ds ? (const void *)jq_batched_kernel<true> : (const void *)jq_batched_kernel<false>;
+  int smem = (int)smem_layout_bytes(wo_slots, ds);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return JQ_ERR_LAUNCH;
   int sms = 0, per = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, jq_batched_kernel, BT, smem) != cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, BT, smem) != cudaSuccess)
     return JQ_ERR_LAUNCH;
   *max_blocks = (size_t)sms * per;
   return JQ_OK;
+}
+
+int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
+                       size_t blocks_data_len, size_t num_blocks, size_t num_major_stages,
+                       uint32_t *out, void *stream) {
+  if (!blocks_start || !blocks_data || !out || num_blocks == 0 || num_major_stages == 0 ||
+      out == blocks_data)
+    return JQ_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(out, blocks_data, blocks_data_len * sizeof(uint32_t),
+                      cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return JQ_ERR_CUDA;
+  const size_t entries = num_blocks * num_major_stages;
+  jq_batched_prepare_kernel<<<(unsigned)entries, BT, 0, st>>>(blocks_start, blocks_data, out,
+                                                               (unsigned)entries);
+  return cudaGetLastError() == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
 }
 
 int jq_simulate_batched(const jq_batch_args *a) {
@@ -606,8 +740,9 @@ int jq_simulate_batched(const jq_batch_args *a) {
   cudaStream_t st = (cudaStream_t)a->stream;
   int dev = 0;
   cudaGetDevice(&dev);
+  const uint32_t wo_slots = a->wo_slots ? a->wo_slots : 256;
   size_t maxg = 0;
-  if (jq_batched_max_blocks(dev, a->wo_slots, &maxg) != JQ_OK || maxg == 0) return JQ_ERR_LAUNCH;
+  if (jq_batched_max_blocks(dev, wo_slots, &maxg) != JQ_OK || maxg == 0) return JQ_ERR_LAUNCH;
   size_t grid = a->grid ? a->grid : maxg;
   if (grid > maxg) return JQ_ERR_TOO_MANY_BLOCKS;
   BatchParams P;
@@ -631,7 +766,7 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.n_po = a->n_po;
   P.wave = a->wave;
   P.record = a->record;
-  P.wo_slots = a->wo_slots ? a->wo_slots : 256;
+  P.wo_slots = wo_slots;
   P.block_list = a->block_list;
   P.block_list_start = a->block_list_start;
   P.part_cycles = a->part_cycles;
@@ -641,10 +776,12 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.slot = 1;
   jq_batched_reset_kernel<<<1, 1, 0, st>>>(P.slot);
   if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
-  int smem = jq_batched_smem_bytes(P.wo_slots);
+  const bool ds = use_double_buffer(P.wo_slots);
+  int smem = (int)smem_layout_bytes(P.wo_slots, ds);
   void *args[] = {&P};
-  cudaError_t e = cudaLaunchCooperativeKernel((void *)jq_batched_kernel, (unsigned)grid, BT, args,
-                                              smem, st);
+  cudaError_t e = cudaLaunchCooperativeKernel(
+      ds ? (void *)jq_batched_kernel<true> : (void *)jq_batched_kernel<false>, (unsigned)grid, BT,
+      args, smem, st);
   return e == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
 }
 

@@ -17,12 +17,13 @@ def per_stream_states(kind, s, cycles, streams, x_init):
     return np.stack(out)  # (S, cycles+1, eff)
 
 
-@pytest.mark.parametrize("kind,nb,split,xprop,lanes", [
-    ("tiny", 8, (5,), False, 1),
-    ("sram", 16, (8,), True, 2),
-    ("soc_mini", 148, (20, 40, 60), True, 1),
+@pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots", [
+    ("tiny", 8, (5,), False, 1, None),
+    ("sram", 16, (8,), True, 2, None),
+    ("sram", 16, (8,), True, 1, 256),  # single-buffered tree state
+    ("soc_mini", 148, (20, 40, 60), True, 1, None),
 ])
-def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes):
+def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slots):
     s = cases.script(kind, nb, split, xprop=xprop)
     cycles = 10
     S = 32 * lanes
@@ -39,7 +40,7 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes):
         want[k] = st.reshape(cycles + 1, eff)
         wsram.append(sram)
     # batched
-    B = batched.BatchedSim(s, lanes, record=True)
+    B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots)
     bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
     B.load_state(bt[0])
     B.reset_sram()
