@@ -148,20 +148,31 @@ typedef struct {
                                       cycles (partition order of the script:
                                       major stage, block, position in block) */
   const uint32_t *part_base;   /* device: index of the first partition of each
-                                  (major stage, block); required with
-                                  part_cycles */
+                                  (major stage, block), from jq_batched_prepare */
+  const uint32_t *gr_sources;  /* device: global-read sources, from
+                                  jq_batched_prepare */
   size_t grid;                 /* CTAs; 0 = all that fit */
   uint64_t barrier_timeout_cycles;
   void *stream;
 } jq_batch_args;
 
-/* Rewrites a script (FlattenedScriptV1 blocks_data, device) into `out`
- * (device, blocks_data_len words, 16-byte aligned) in the batched
- * interpreter's layout: same size and partition offsets, boomerang chunks
- * reordered per thread.  Asynchronous on `stream`.  Run once per script. */
+/* Prepares a script (FlattenedScriptV1, device arrays) for the batched
+ * interpreter; run once per script, synchronizes `stream`.  Outputs (device):
+ *   out         blocks_data_len words, 16-byte aligned: the script in the
+ *               batched layout (same size and partition offsets, boomerang
+ *               chunks reordered per thread);
+ *   part_base   num_blocks * num_major_stages words: index of the first
+ *               partition of each (major stage, block), partitions numbered
+ *               in script order;
+ *   gr_sources  jq_batched_gr_words(num_partitions) words: the source signal
+ *               of each global-read position of each partition.
+ * JQ_ERR_INVALID_ARG when the script holds other than num_partitions
+ * partitions. */
+size_t jq_batched_gr_words(size_t num_partitions);
 int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
                        size_t blocks_data_len, size_t num_blocks, size_t num_major_stages,
-                       uint32_t *out, void *stream);
+                       size_t num_partitions, uint32_t *out, uint32_t *part_base,
+                       uint32_t *gr_sources, void *stream);
 int jq_simulate_batched(const jq_batch_args *a);
 /* Synchronizes `stream`; JQ_OK or the kernel's recorded error. */
 int jq_batched_status(void *stream);

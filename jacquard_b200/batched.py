@@ -25,7 +25,7 @@ class BatchArgs(ctypes.Structure):
                 ("input_regions", vp), ("n_input_regions", ctypes.c_uint32),
                 ("po_signals", vp), ("n_po", ctypes.c_uint32), ("wave", vp), ("record", vp),
                 ("wo_slots", ctypes.c_uint32), ("block_list", vp), ("block_list_start", vp),
-                ("part_cycles", vp), ("part_base", vp),
+                ("part_cycles", vp), ("part_base", vp), ("gr_sources", vp),
                 ("grid", ctypes.c_size_t),
                 ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp)]
 
@@ -39,9 +39,11 @@ def lib():
         L.jq_batched_status.argtypes = [vp]
         L.jq_batched_max_blocks.restype = ctypes.c_int
         L.jq_batched_max_blocks.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_size_t)]
+        L.jq_batched_gr_words.restype = ctypes.c_size_t
+        L.jq_batched_gr_words.argtypes = [ctypes.c_size_t]
         L.jq_batched_prepare.restype = ctypes.c_int
         L.jq_batched_prepare.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
-                                         vp, vp]
+                                         ctypes.c_size_t, vp, vp, vp, vp]
         L._jq_batched_typed = True
     return L
 
@@ -126,12 +128,24 @@ class BatchedSim:
         self.lanes = lanes
         self.device = torch.device(device)
         self.ds = sim.DeviceScript(script, self.device)
-        # the kernel reads the script in its own prepared layout
+        # the kernel reads the script in its own prepared layout, with the
+        # global-read sources resolved once
+        L = lib()
+        n_parts = getattr(script, "num_partitions", None)
+        if n_parts is None:
+            n_parts = len(script.stage_block_part)
+        self.num_partitions = int(n_parts)
         self.prepared = torch.empty_like(self.ds.blocks_data)
-        rc = lib().jq_batched_prepare(self.ds.blocks_start.data_ptr(), self.ds.blocks_data.data_ptr(),
-                                      self.ds.blocks_data.numel(), self.ds.num_blocks,
-                                      self.ds.num_major_stages, self.prepared.data_ptr(),
-                                      torch.cuda.current_stream(self.device).cuda_stream)
+        self.part_base_dev = torch.empty(self.ds.num_blocks * self.ds.num_major_stages,
+                                         dtype=torch.int32, device=self.device)
+        self.gr_sources = torch.empty(L.jq_batched_gr_words(self.num_partitions), dtype=torch.int32,
+                                      device=self.device)
+        rc = L.jq_batched_prepare(self.ds.blocks_start.data_ptr(), self.ds.blocks_data.data_ptr(),
+                                  self.ds.blocks_data.numel(), self.ds.num_blocks,
+                                  self.ds.num_major_stages, self.num_partitions,
+                                  self.prepared.data_ptr(), self.part_base_dev.data_ptr(),
+                                  self.gr_sources.data_ptr(),
+                                  torch.cuda.current_stream(self.device).cuda_stream)
         if rc:
             raise RuntimeError("jq_batched_prepare: " + sim.lib().jq_strerror(rc).decode())
         self.eff = getattr(script, "effective_words", None) or \
@@ -202,17 +216,12 @@ class BatchedSim:
                       record_buf.data_ptr() if record_buf is not None else None,
                       self.wo_slots, self.block_list.data_ptr(), self.block_list_start.data_ptr(),
                       part_cycles.data_ptr() if part_cycles is not None else None,
-                      self._part_base().data_ptr() if part_cycles is not None else None,
+                      self.part_base_dev.data_ptr(), self.gr_sources.data_ptr(),
                       self.grid, 0,
                       stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
         rc = L.jq_simulate_batched(ctypes.byref(a))
         if rc:
             raise RuntimeError("jq_simulate_batched: " + sim.lib().jq_strerror(rc).decode())
-
-    def _part_base(self):
-        if getattr(self, "_pb", None) is None:
-            self._pb = torch.from_numpy(self.part_base().view(np.int32)).to(self.device)
-        return self._pb
 
     def status(self, stream=None):
         s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream

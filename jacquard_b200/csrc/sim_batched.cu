@@ -25,6 +25,7 @@
 #include "sim_common.cuh"
 
 #include <cstdio>
+#include <cstdlib>
 
 namespace jqk {
 
@@ -55,6 +56,8 @@ struct BatchParams {
   const uint32_t *block_list_start;  // num_major_stages + 1 offsets
   unsigned long long *part_cycles;   // optional per-partition SM-clock totals
   const uint32_t *part_base;         // first partition index of (stage, block)
+  const uint32_t *gr_sources;        // per partition: source signal of each of
+                                     // the 8192 global-read positions
   uint64_t timeout;
   int slot;
 };
@@ -153,7 +156,7 @@ template <bool DS>
 __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, uint32_t *chunks,
                          uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                          const uint32_t *in, uint32_t *out, uint32_t lane, uint32_t pid0,
-                         bool &failed) {
+                         bool &failed, uint32_t &next_ticket, bool &have_next) {
   const int t = threadIdx.x;
   const size_t lane_base = (size_t)lane * P.sig_per_snap;
   constexpr bool ds = DS;
@@ -165,6 +168,13 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     __syncthreads();
     const long long t_start = clock64();
     if (t < 256) sh.meta[t] = __ldg(script + off + t);
+    // global-read sources of this partition (only used when it exists)
+    uint32_t e[16];
+    {
+      const uint32_t *src = P.gr_sources + (size_t)pid * 8192;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) e[k] = __ldg(src + t + BT * k);
+    }
     __syncthreads();
     const uint32_t ns = sh.meta[0];
     if (!ns) break;
@@ -175,7 +185,10 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     const uint32_t xsig = sh.meta[9] * 32u;
     const uint32_t *gr = script + off + 256;
     const uint32_t *ch0 = gr + 512 * (size_t)R;
-    const uint32_t nchunks = ns + 2;
+    // chunk sequence: the ns boomerang stages, the SRAM/duplicate chunk
+    // (only when the partition has SRAMs or duplicates), the clock-enable chunk
+    const bool has_sram = (num_srams | num_dup) != 0;
+    const uint32_t nchunks = ns + (has_sram ? 2 : 1);
 
     // chunk 0 -> buffer 0 (the previous item/partition finished with both)
     if (t == 0) {
@@ -183,55 +196,13 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
       tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
     }
 
-    // ---- global read into tree buffer 0, in two phases so that the loads
-    // overlap:
-    // (a) thread t < 256 enumerates its (idx, mask) bits and stores, at the
-    //     destination position, the source signal (bit 31 = current-cycle
-    //     staged IO) or NONE for the unfilled tail; positions follow the
-    //     kernel's append order (first appended bit ends up most significant);
-    // (b) all threads load their 16 positions with independent loads.
-    uint32_t *Sv = reinterpret_cast<uint32_t *>(Sb0);  // staging: .x words
-    if (t < 256) {
-      uint2 pr[16];
-#pragma unroll
-      for (int r = 0; r < 16; ++r)
-        pr[r] = (uint32_t)r < R ? ldg2(gr + 512 * r + 2 * t) : make_uint2(0, 0);
-      uint32_t total = 0;
-#pragma unroll
-      for (int r = 0; r < 16; ++r) total += __popc(pr[r].y);
-      for (uint32_t r = 16; r < R; ++r) total += __popc(__ldg(gr + 512 * r + 2 * t + 1));
-      uint32_t i = 0;
-#pragma unroll
-      for (int r = 0; r < 16; ++r) {
-        uint32_t m = pr[r].y;
-        const uint32_t stg = pr[r].x & 0x80000000u;
-        const uint32_t w = pr[r].x & 0x7fffffffu;
-        while (m) {
-          const uint32_t k = __ffs(m) - 1;
-          m &= m - 1;
-          Sv[2 * sw(32 * t + (total - 1 - i))] = stg | (w * 32 + k);
-          ++i;
-        }
-      }
-      for (uint32_t r = 16; r < R; ++r) {
-        const uint2 im = ldg2(gr + 512 * r + 2 * t);
-        uint32_t m = im.y;
-        const uint32_t stg = im.x & 0x80000000u;
-        const uint32_t w = im.x & 0x7fffffffu;
-        while (m) {
-          const uint32_t k = __ffs(m) - 1;
-          m &= m - 1;
-          Sv[2 * sw(32 * t + (total - 1 - i))] = stg | (w * 32 + k);
-          ++i;
-        }
-      }
-      for (uint32_t k = total; k < 32; ++k) Sv[2 * sw(32 * t + k)] = 0xffffffffu;
-    }
-    __syncthreads();
+    // ---- global read into tree buffer 0.  The source signal of every
+    // position (the kernel's bit-append order, resolved once per script by
+    // jq_batched_prepare; bit 31 = current-cycle staged IO, all ones = none)
+    // was loaded at the top of the partition; 32 independent state loads per
+    // thread follow.
     {
-      uint32_t e[16], v[16], vx[16];
-#pragma unroll
-      for (int k = 0; k < 16; ++k) e[k] = Sv[2 * sw(t + BT * k)];
+      uint32_t v[16], vx[16];
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
         v[k] = 0;
@@ -264,8 +235,9 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
       // the previous chunk, so the next chunk can be issued right away.
       if (t == 0 && ci + 1 < nchunks) {
         mbar_expect_tx(&sh.bar[b ^ 1], CHUNK_BYTES);
-        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * (ci + 1),
-                    CHUNK_BYTES, &sh.bar[b ^ 1]);
+        const uint32_t nxt = (!has_sram && ci + 1 == ns) ? ns + 1 : ci + 1;  // script chunk
+        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, CHUNK_BYTES,
+                    &sh.bar[b ^ 1]);
       }
       uint32_t &uses = b ? uses1 : uses0;
       // warp-uniform, so the shuffles below run with full warps
@@ -357,7 +329,8 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         if (t < 32) {
           uint2 h = t < 16 ? Sn[sw(16 + t)] : make_uint2(0, 0);
           uint32_t hv = h.x, hx = h.y;
-#pragma unroll
+          // rolled: this serial section runs in one warp, keep its code short
+#pragma unroll 1
           for (int m = 0; m < 4; ++m) {
             const uint32_t len = 8u >> m;
             const uint32_t bb = __shfl_sync(0xffffffffu, hv, (t + len) & 31);
@@ -380,7 +353,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
           if ((hook >> 8) == ci) WO[slot * 32 + lane_i] = Sn[sw((hook & 255u) * 32 + lane_i)];
         }
-      } else if (ci == ns) {
+      } else if (has_sram && ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports
         JQ_FAIL_IF(!ok)  // hooks done, chunk landed
         uint2 *St = Sb0;  // staging (the last stage's hooks are done)
@@ -440,6 +413,12 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         // ---------------- clock-enable permutation and commit (4 words per
         // thread in flight)
         JQ_FAIL_IF(!ok)
+        // the item's last commit: take the next work ticket now, so its
+        // latency overlaps the commit
+        if (t == 0 && is_last) {
+          next_ticket = atomicAdd(&g_ticket[P.slot], 1u);
+          have_next = true;
+        }
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
         for (uint32_t q0 = t; q0 < nq; q0 += 4 * BT) {
@@ -535,17 +514,21 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
                                          : P.num_blocks;
       const uint32_t items = nblk * P.lanes;
+      uint32_t next_ticket = 0;
+      bool have_next = false;
       for (;;) {
         __syncthreads();
-        if (t == 0) sh.ticket = atomicAdd(&g_ticket[P.slot], 1u);
+        if (t == 0) sh.ticket = have_next ? next_ticket : atomicAdd(&g_ticket[P.slot], 1u);
         __syncthreads();
+        have_next = false;
         const uint32_t tk = sh.ticket;
         if (tk >= items) break;
         const uint32_t bi = tk / P.lanes, lane = tk % P.lanes;
         const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
         const uint32_t *script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
-        const uint32_t pid0 = P.part_base ? P.part_base[(size_t)ms * P.num_blocks + blk] : 0u;
-        run_item<DS>(P, sh, S, WO, chunks, uses0, uses1, script, in, out, lane, pid0, failed);
+        const uint32_t pid0 = P.part_base[(size_t)ms * P.num_blocks + blk];
+        run_item<DS>(P, sh, S, WO, chunks, uses0, uses1, script, in, out, lane, pid0, failed,
+                     next_ticket, have_next);
         if (failed) {
           if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
           return;
@@ -603,18 +586,43 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 // clock-enable chunks get their shuffle entries in q order.  Metadata, global
 // read sections and sizes are unchanged, so blocks_start stays valid.  One
 // CTA per (major stage, block) entry walks its partition list.
-__global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(const size_t *blocks_start,
-                                                                const uint32_t *src,
-                                                                uint32_t *dst, unsigned entries) {
+__global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
+    const size_t *blocks_start, const uint32_t *src, uint32_t *dst, unsigned entries,
+    const uint32_t *part_base, uint32_t *gr_sources, size_t num_partitions) {
   const unsigned e = blockIdx.x;
   if (e >= entries) return;
   const uint32_t t = threadIdx.x;
   const uint32_t u = residue(t);
   size_t off = blocks_start[e];
+  size_t pid = part_base[e];
   for (;;) {
     const uint32_t ns = src[off];
-    if (!ns) break;
+    if (!ns || pid >= num_partitions) break;
     const uint32_t is_last = src[off + 1], R = src[off + 6];
+    // global-read sources: thread t < 256 appends its masked bits round by
+    // round, walking each mask from the lowest set bit; the first appended
+    // bit ends up most significant, i.e. at position 32t + total - 1
+    // (csrc/kernel_v1_impl.cuh:87-154).  Unfilled positions get all ones.
+    if (t < 256) {
+      const uint32_t *gr = src + off + 256;
+      uint32_t *G = gr_sources + pid * 8192 + 32 * t;
+      uint32_t total = 0;
+      for (uint32_t r = 0; r < R; ++r) total += __popc(gr[512 * r + 2 * t + 1]);
+      if (total > 32) total = 32;  // at most 32 bits per thread (script validator)
+      uint32_t i = 0;
+      for (uint32_t r = 0; r < R; ++r) {
+        uint32_t m = gr[512 * r + 2 * t + 1];
+        const uint32_t idx = gr[512 * r + 2 * t];
+        const uint32_t stg = idx & 0x80000000u, w = idx & 0x7fffffffu;
+        while (m && i < 32) {
+          const uint32_t k = __ffs(m) - 1;
+          m &= m - 1;
+          G[total - 1 - i] = stg | (w * 32 + k);
+          ++i;
+        }
+      }
+      for (uint32_t k = total; k < 32; ++k) G[k] = 0xffffffffu;
+    }
     const uint32_t *ch = src + off + 256 + 512 * (size_t)R;
     uint32_t *dch = dst + off + 256 + 512 * (size_t)R;
     for (uint32_t ci = 0; ci < ns + 2; ++ci) {
@@ -665,8 +673,26 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(const size_t *bl
       }
     }
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    ++pid;
     if (is_last) break;
   }
+}
+
+// Number of partitions in each (major stage, block) entry's list.
+__global__ void jq_batched_count_kernel(const size_t *blocks_start, const uint32_t *src,
+                                        uint32_t *counts, unsigned entries) {
+  const unsigned e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= entries) return;
+  size_t off = blocks_start[e];
+  uint32_t n = 0;
+  for (;;) {
+    const uint32_t ns = src[off];
+    if (!ns) break;
+    ++n;
+    if (src[off + 1]) break;
+    off += 256 + 512 * (size_t)src[off + 6] + STAGE_WORDS * ((size_t)ns + 2);
+  }
+  counts[e] = n;
 }
 
 }  // namespace jqk
@@ -716,20 +742,51 @@ int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
   return JQ_OK;
 }
 
+size_t jq_batched_gr_words(size_t num_partitions) { return (num_partitions + 1) * 8192; }
+
 int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
                        size_t blocks_data_len, size_t num_blocks, size_t num_major_stages,
-                       uint32_t *out, void *stream) {
-  if (!blocks_start || !blocks_data || !out || num_blocks == 0 || num_major_stages == 0 ||
-      out == blocks_data)
+                       size_t num_partitions, uint32_t *out, uint32_t *part_base,
+                       uint32_t *gr_sources, void *stream) {
+  if (!blocks_start || !blocks_data || !out || !part_base || !gr_sources || num_blocks == 0 ||
+      num_major_stages == 0 || out == blocks_data)
     return JQ_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  if (cudaMemcpyAsync(out, blocks_data, blocks_data_len * sizeof(uint32_t),
-                      cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return JQ_ERR_CUDA;
   const size_t entries = num_blocks * num_major_stages;
-  jq_batched_prepare_kernel<<<(unsigned)entries, BT, 0, st>>>(blocks_start, blocks_data, out,
-                                                               (unsigned)entries);
-  return cudaGetLastError() == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
+  jq_batched_count_kernel<<<(unsigned)((entries + 255) / 256), 256, 0, st>>>(
+      blocks_start, blocks_data, part_base, (unsigned)entries);
+  if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
+  uint32_t *h = (uint32_t *)malloc(entries * sizeof(uint32_t));
+  if (!h) return JQ_ERR_INVALID_ARG;
+  if (cudaMemcpyAsync(h, part_base, entries * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    free(h);
+    return JQ_ERR_CUDA;
+  }
+  // counts -> first partition index of each entry (script order)
+  size_t total = 0;
+  for (size_t e = 0; e < entries; ++e) {
+    const uint32_t c = h[e];
+    h[e] = (uint32_t)total;
+    total += c;
+  }
+  int rc = JQ_OK;
+  if (total != num_partitions) {
+    rc = JQ_ERR_INVALID_ARG;
+  } else if (cudaMemcpyAsync(part_base, h, entries * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                             st) != cudaSuccess ||
+             cudaMemcpyAsync(out, blocks_data, blocks_data_len * sizeof(uint32_t),
+                             cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+    rc = JQ_ERR_CUDA;
+  } else {
+    jq_batched_prepare_kernel<<<(unsigned)entries, BT, 0, st>>>(
+        blocks_start, blocks_data, out, (unsigned)entries, part_base, gr_sources, num_partitions);
+    if (cudaGetLastError() != cudaSuccess) rc = JQ_ERR_LAUNCH;
+    else if (cudaStreamSynchronize(st) != cudaSuccess) rc = JQ_ERR_CUDA;
+  }
+  free(h);
+  return rc;
 }
 
 int jq_simulate_batched(const jq_batch_args *a) {
@@ -771,7 +828,8 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.block_list_start = a->block_list_start;
   P.part_cycles = a->part_cycles;
   P.part_base = a->part_base;
-  if (P.part_cycles && !P.part_base) return JQ_ERR_INVALID_ARG;
+  P.gr_sources = a->gr_sources;
+  if (!P.part_base || !P.gr_sources) return JQ_ERR_INVALID_ARG;
   P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
   P.slot = 1;
   jq_batched_reset_kernel<<<1, 1, 0, st>>>(P.slot);
