@@ -37,18 +37,45 @@ std::string validate_script(const FlatScript &s, size_t state_words) {
       size_t need = NT + 2 * (size_t)NT * R + 5120 * ((size_t)ns + 2);
       if (pi + need > end) { err << "block " << bi << ": partition overruns block"; return err.str(); }
       const uint32_t *g = m + NT;
-      for (uint32_t r = 0; r < R; ++r)
-        for (uint32_t t = 0; t < NT; ++t) {
+      for (uint32_t t = 0; t < NT; ++t) {
+        uint32_t bits = 0;
+        for (uint32_t r = 0; r < R; ++r) {
           uint32_t idx = g[r * 2 * NT + 2 * t], mask = g[r * 2 * NT + 2 * t + 1];
           if (!mask) continue;
+          bits += (uint32_t)__builtin_popcount(mask);
           if ((idx & 0x7fffffffu) >= rio) { err << "block " << bi << ": global read index"; return err.str(); }
         }
+        // a thread appends at most 32 bits (one state word)
+        if (bits > 32) { err << "block " << bi << ": global read bits per thread"; return err.str(); }
+      }
       const uint32_t *st = g + 2 * (size_t)NT * R;
       for (uint32_t k = 0; k < ns + 2; ++k) {
         const uint32_t *ch = st + 5120 * (size_t)k;
         for (int q = 0; q < 4096; ++q) {
           uint32_t w = ch[q];
           if ((w & 0xffff) >= 8192 || (w >> 16) >= 8192) { err << "block " << bi << ": shuffle index"; return err.str(); }
+        }
+      }
+      // SRAM/duplicate and clock-enable permutations read writeout slots:
+      // every used entry must point below num_ios * 32
+      for (uint32_t k = ns; k < ns + 2; ++k) {
+        const uint32_t *ch = st + 5120 * (size_t)k;
+        const uint32_t nq = (k == ns ? nsr * 4 + nd : nio) * 32;
+        for (uint32_t q = 0; q < nq; ++q) {
+          const uint32_t T = q >> 5, kk = q & 31;
+          const uint32_t w = ch[(kk >> 3) * 1024 + T * 4 + ((kk >> 1) & 3)];
+          const uint32_t e = (kk & 1) ? (w >> 16) : (w & 0xffff);
+          if (e >= nio * 32) { err << "block " << bi << ": writeout permutation index"; return err.str(); }
+        }
+      }
+      // SRAM port addresses are 13 bits: bits 13..15 of the read and write
+      // address words must be forced to 0 (set0 on, inversion off)
+      {
+        const uint32_t *F = st + 5120 * (size_t)ns + 4096;
+        for (uint32_t i = 0; i < nsr; ++i) {
+          const uint32_t inv = F[4 * (4 * i) + 0], set0 = F[4 * (4 * i) + 1];
+          const uint32_t hi = 0xe000e000u;
+          if ((set0 & hi) != hi || (inv & hi) != 0) { err << "block " << bi << ": SRAM address bits"; return err.str(); }
         }
       }
       pi += need;

@@ -72,6 +72,50 @@ def test_validator_accepts_built_scripts_and_rejects_corruption():
     assert validate(s, rio=1)[0] != 0
 
 
+def partitions(s):
+    """(offset, ns, R, nio, nsr, nd) of every partition of a script."""
+    bd = s.blocks_data
+    out = []
+    for b in range(s.num_blocks * s.num_major_stages):
+        off = int(s.blocks_start[b])
+        while int(bd[off]):
+            ns, R = int(bd[off]), int(bd[off + 6])
+            out.append((off, ns, R, int(bd[off + 2]), int(bd[off + 4]), int(bd[off + 7])))
+            last = int(bd[off + 1])
+            off += 256 + 512 * R + 5120 * (ns + 2)
+            if last:
+                break
+    return out
+
+
+def test_validator_rejects_out_of_range_kernel_indices():
+    """Indices the kernels dereference without further checks: more than 32
+    global-read bits for one thread, writeout permutation entries past
+    num_ios*32, SRAM address bits 13..15 not forced to 0."""
+    s = cases.script("sram", 16, (8,))
+    parts = partitions(s)
+    off, ns, R, nio, nsr, nd = next(p for p in parts if p[2] > 0)
+    # global read: 33 bits for thread 0 (two full masks)
+    bad = s.blocks_data.copy()
+    bad[off + 256: off + 256 + 2] = (0, 0xFFFFFFFF)
+    if R > 1:
+        bad[off + 256 + 512: off + 256 + 512 + 2] = (0, 1)
+        assert validate(s, data=bad)[0] != 0
+    # clock-enable permutation entry 0 (q = 0) pointing at slot nio
+    bad = s.blocks_data.copy()
+    ck = off + 256 + 512 * R + 5120 * (ns + 1)
+    bad[ck] = (bad[ck] & 0xFFFF0000) | (nio * 32)
+    r, msg = validate(s, data=bad)
+    assert r != 0 and "permutation" in msg
+    # SRAM read address bit 13 left live
+    off, ns, R, nio, nsr, nd = next(p for p in parts if p[4] > 0)
+    bad = s.blocks_data.copy()
+    fl = off + 256 + 512 * R + 5120 * ns + 4096
+    bad[fl + 1] &= ~np.uint32(1 << 13)
+    r, msg = validate(s, data=bad)
+    assert r != 0 and "SRAM address" in msg
+
+
 def test_xprop_classification_marks_partitions():
     s = cases.script("sram", 16, (8,), xprop=True)
     assert s.partition_x_capable.any()
