@@ -27,11 +27,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 sys.path.insert(0, os.path.join(HERE, "tests"))
 
-LEVEL_SPLIT = tuple(range(5, 80, 5))
+LEVEL_SPLIT = tuple(range(4, 80, 4))
 TARGET_CONE = 6000
 RESET_CYCLES = 16
 P_TOGGLE = 0.25
 METRIC = "stimulus-cycles/s bit-exact: batched+learned vs plain kernel vs CPU, 1 B200"
+
+
+# DRAM bytes (read + write) per simulated cycle of the 256-stream batched
+# workload: dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
+# jq_batched_kernel (a 4-cycle launch after 3 warm-up launches), divided by
+# its 4 cycles; traffic grows in proportion to the cycle count.
+BATCHED_DRAM_BYTES_PER_CYCLE = (646.699264e6 + 264.490240e6) / 4
 
 
 def peaks():
@@ -456,7 +463,10 @@ def main():
                            "cycles_per_step": r["cycles_per_step"], "l2": "inputs larger than L2 (snapshot window + script)",
                            **r["design"]},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
+                             "frac": achieved / peak, "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_launch": r["bytes_per_cycle"] * r["cycles_per_step"],
+                             "traffic": (BATCHED_DRAM_BYTES_PER_CYCLE * r["cycles_per_step"]
+                                         if args.mode == "batched" and args.clusters == 512 else None)},
                 "cpu_baseline": {"value": cpu_v, "unit": "stimulus-cycles/s", "cores": 1,
                                  "kind": "port",
                                  "sample": f"{args.cpu_cycles} cycles x 1 stream, {cpu_dt:.1f} s"},

@@ -1,7 +1,7 @@
 """Parity at the benchmark's full size: the 2M-gate SoC design (2^21 clustered
 ANDs + reset gates, depth 80, 200k DFFs, 16 SRAMs 1024x32, X-propagation,
 every DFF and SRAM bit X at start), scripted as the benchmark scripts it
-(148 blocks, level split every 5 levels, 6000-gate partitions).
+(148 blocks, level split every 4 levels, 6000-gate partitions).
 
 - The batched interpreter over 256 streams against the plain interpreter run
   stream by stream, every snapshot and the SRAM contents of every stream; two
@@ -23,7 +23,7 @@ from jacquard_b200 import batched, frontend, sim, state
 
 pytestmark = pytest.mark.gpu
 
-SPLIT = tuple(range(5, 80, 5))
+SPLIT = tuple(range(4, 80, 4))
 CYCLES = 12
 LANES = 8
 THREADS = os.cpu_count() or 1
