@@ -233,6 +233,31 @@ int jq_mlp_train_step(const jq_mlp_step_args *a);
 #define JQ_MLP_NOALLOC_MAX_CTAS 16
 int jq_mlp_train_step_noalloc(const jq_mlp_step_args *a);
 
+/* ------------------------------------------------------------------------ */
+/* Output transitions for waveform writers (no counterpart in the reference,
+ * whose writer walks every output of every snapshot on the host,
+ * src/sim/vcd_io.rs:758-946).  Walks snapshots first_snapshot ..
+ * first_snapshot+num_snapshots-1 of `states` (device, snapshot_words words
+ * each).  Each output j has a code: 3 when its X bit is set (X word
+ * xmask_offset words after its value word, when xmask_offset != 0), else its
+ * value bit.  Constant outputs, with out_pos[j] = 0xFFFFFFFF, take
+ * out_const[j] (0 when out_const is NULL).  A transition is a code that
+ * differs from the previous snapshot's (2 = unknown before the first).
+ *
+ * Outputs (device):
+ *   counts[s]    transitions of walk step s;
+ *   offsets[s]   their start, with offsets[num_snapshots] = total;
+ *   transitions  j | code << 30, in (snapshot, output) order, capacity entries;
+ *   arrivals     (optional) the low 16 bits of each transition's arrival
+ *                word, arrival_offset words after the value word.
+ * *total gets the number of transitions.  Returns JQ_ERR_EVENT_OVERFLOW when
+ * it exceeds capacity (capacity 0 only counts).  Synchronizes `stream`. */
+int jq_output_transitions(const uint32_t *states, size_t first_snapshot, size_t num_snapshots,
+                          size_t snapshot_words, size_t xmask_offset, size_t arrival_offset,
+                          const uint32_t *out_pos, const uint32_t *out_const, uint32_t n_out,
+                          uint32_t *counts, unsigned long long *offsets, uint32_t *transitions,
+                          uint32_t *arrivals, size_t capacity, size_t *total, void *stream);
+
 /* Human-readable text for a status code. */
 const char *jq_strerror(int code);
 

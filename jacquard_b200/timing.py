@@ -134,26 +134,54 @@ def process_events(events, count, capacity, stats, builder=None, resolver=None):
                              "arrival_ps": arr, "constraint_ps": cons, "slack_ps": slack})
 
 
+def constraint_buffer(design, script, clock_ps, setup_ps, hold_ps, clock_arrival_ps):
+    """Timing constraint buffer [clock_ps, per-word setup<<16 | hold] for every
+    DFF of a design (build_timing_constraint_buffer, src/flatten.rs:1891-1924,
+    with the clock-arrival fold of :97-123): per-DFF setup/hold/clock arrival
+    arrays (or scalars), folded to the per-word minimum."""
+    import ctypes
+    from .frontend import _lib
+    n = int(design.num_dffs)
+    su = np.broadcast_to(np.asarray(setup_ps, np.uint16), (n,)).copy()
+    ho = np.broadcast_to(np.asarray(hold_ps, np.uint16), (n,)).copy()
+    ca = np.broadcast_to(np.asarray(clock_arrival_ps, np.int16), (n,)).copy()
+    pos = np.ascontiguousarray(script.dff_data_pos, dtype=np.uint32)
+    out = np.zeros(script.reg_io_state_size, np.uint32)
+    clk = ctypes.c_uint32()
+    vp = ctypes.c_void_p
+    rc = _lib().jqf_constraint_buffer(ctypes.c_uint32(script.reg_io_state_size),
+                                      ctypes.c_uint64(clock_ps), ctypes.c_size_t(n),
+                                      su.ctypes.data_as(vp), ho.ctypes.data_as(vp),
+                                      ca.ctypes.data_as(vp), pos.ctypes.data_as(vp),
+                                      ctypes.byref(clk), out.ctypes.data_as(vp))
+    if rc:
+        raise ValueError("constraint buffer: bad arguments")
+    return np.concatenate([[np.uint32(clk.value)], out]).astype(np.uint32)
+
+
 def new_stats():
     return {"setup_violations": 0, "hold_violations": 0, "events_dropped": 0}
 
 
 def run_timed(ds, states, cycles, state_size, sram, sram_x, constraints, window, capacity,
-              arrival_state_offset, builder=None, resolver=None, stream=None):
+              arrival_state_offset, builder=None, resolver=None, stream=None, first_cycle=0,
+              stats=None, events=None):
     """Timed simulation in windows of `window` cycles on the plain interpreter;
     each window's event buffer is drained into the stats and report.  `states`
-    holds all (cycles+1) snapshots on the device.  Returns the stats dict."""
+    holds the (cycles+1) snapshots on the device; events are numbered from
+    `first_cycle`.  `stats` (accumulated) and `events` (a buffer of
+    `capacity` records) may be passed in to reuse them.  Returns the stats."""
     import torch
     from . import sim
-    stats = new_stats()
-    ev = sim.new_event_buffer(capacity, device=states.device)
+    stats = new_stats() if stats is None else stats
+    ev = sim.new_event_buffer(capacity, device=states.device) if events is None else events
     for c0 in range(0, cycles, window):
         n = min(window, cycles - c0)
         ev[:2].zero_()
         view = states[c0 * state_size:]
         sim.simulate(ds, view, n, state_size, sram, sram_x, constraints=constraints, events=ev,
                      event_capacity=capacity, arrival_state_offset=arrival_state_offset,
-                     first_cycle=c0, stream=stream)
+                     first_cycle=first_cycle + c0, stream=stream)
         rc = sim.status(stream)
         if rc not in (0,):
             raise RuntimeError(sim.lib().jq_strerror(rc).decode())

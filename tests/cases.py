@@ -59,20 +59,8 @@ def constraint_buffer(kind, s, clock_ps=10_000, setup=30, hold=10, seed=5):
 
 
 def constraint_buffer_for(d, s, clock_ps=10_000, setup=30, hold=10, seed=5):
-    """Same, for a design object: jqf_constraint_buffer over every DFF."""
-    import ctypes
-    from jacquard_b200.frontend import _lib
+    """Same, for a design object (every DFF: setup, hold, clock arrival U[0,300])."""
+    from jacquard_b200 import timing
     rng = np.random.default_rng(seed)
-    n = int(d.num_dffs)
-    su = np.full(n, setup, np.uint16)
-    ho = np.full(n, hold, np.uint16)
-    ca = rng.integers(0, 301, size=n).astype(np.int16)
-    pos = np.ascontiguousarray(s.dff_data_pos, dtype=np.uint32)
-    out = np.zeros(s.reg_io_state_size, np.uint32)
-    clk = ctypes.c_uint32()
-    _lib().jqf_constraint_buffer(ctypes.c_uint32(s.reg_io_state_size), ctypes.c_uint64(clock_ps),
-                                 ctypes.c_size_t(n), su.ctypes.data_as(ctypes.c_void_p),
-                                 ho.ctypes.data_as(ctypes.c_void_p), ca.ctypes.data_as(ctypes.c_void_p),
-                                 pos.ctypes.data_as(ctypes.c_void_p), ctypes.byref(clk),
-                                 out.ctypes.data_as(ctypes.c_void_p))
-    return np.concatenate([[np.uint32(clk.value)], out]).astype(np.uint32)
+    ca = rng.integers(0, 301, size=int(d.num_dffs)).astype(np.int16)
+    return timing.constraint_buffer(d, s, clock_ps, setup, hold, ca)
