@@ -32,6 +32,14 @@ TARGET_CONE = 6000
 RESET_CYCLES = 16
 P_TOGGLE = 0.25
 METRIC = "stimulus-cycles/s bit-exact: batched+learned vs plain kernel vs CPU, 1 B200"
+SOC = "soc-2M: 2^21 clustered ANDs + reset gates, depth 80, 200k DFF, 16 SRAM 1024x32, X-prop"
+WORKLOADS = {
+    "batched": SOC,
+    "plain": SOC,
+    "timed": SOC + ", per-pin delays U[20,200] ps, setup 30 / hold 10 ps, 10 ns clock, "
+                   "DFF clock arrival U[0,300] ps, arrivals + setup/hold events drained per window",
+    "multi": "12 SoC-family designs, 50k-4M AND nodes log-uniform, X-prop, one graph-captured launch",
+}
 
 
 # DRAM bytes (read + write) per simulated cycle of the 256-stream batched
@@ -359,6 +367,157 @@ def run_mine_batched(args, rank, world):
                 script=s, d=d)
 
 
+def run_mine_timed(args, rank, world):
+    """Timed path on the plain interpreter: the SoC netlist with per-AND-pin
+    delays U[20,200] ps (rise = fall), setup 30 / hold 10 ps, 10 ns clock,
+    per-DFF clock arrival U[0,300] ps, X-prop, arrivals on.  One step = one
+    window of cycles plus the drain of its setup/hold events into the
+    timing report."""
+    import torch
+    from jacquard_b200 import sim, state, timing
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
+    rng = np.random.default_rng(3)
+    n = d.num_pins + 1
+    r = rng.integers(20, 201, size=n).astype(np.uint32)
+    r[d.kind != 1] = 0
+    d.set_delays(r, r)
+    nb = min(sim.max_blocks(dev.index), 148 * 3)
+    s = build_script(d, nb)
+    zero = np.zeros(n, np.uint32)
+    d.set_delays(zero, zero)
+    s.enable_timing_arrivals()
+    rio = s.reg_io_state_size
+    W = args.window
+    cycles = W * (args.steps + args.warmup)
+    vals = state.stimulus_inputs(s, d, cycles, 100 + rank, P_TOGGLE, RESET_CYCLES)
+    host = state.expand_states_for_arrivals(state.expand_states_for_xprop(state.pack_inputs(s, vals), s), s)
+    host[0, rio:2 * rio] = state.xmask_all_state_x(s)
+    eff = host.shape[1]
+    ca = np.random.default_rng(5).integers(0, 301, size=int(d.num_dffs)).astype(np.int16)
+    cons = sim.u32_to_dev(timing.constraint_buffer(d, s, 10_000, 30, 10, ca), dev)
+    host_pin = torch.from_numpy(np.ascontiguousarray(host).reshape(-1).view(np.int32)).pin_memory()
+    st = torch.empty(host_pin.numel(), dtype=torch.int32, device=dev)
+    st.copy_(host_pin)
+    ds = sim.DeviceScript(s, dev)
+    n_sram = max(1, s.sram_storage_size)
+    sram = torch.zeros(n_sram, dtype=torch.int32, device=dev)
+    sram_x = torch.full((n_sram,), -1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    cap = 1 << 20
+    stats = timing.new_stats()
+    ev = sim.new_event_buffer(cap, device=dev)
+
+    def window(c0):
+        timing.run_timed(ds, st[c0 * eff:], W, eff, sram, sram_x, cons, W, cap,
+                         s.arrival_state_offset, stream=stream, first_cycle=c0, stats=stats,
+                         events=ev)
+
+    for k in range(args.warmup):
+        window(k * W)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as ck:
+        timed_region_edge(world)
+        t0.record(stream)
+        for k in range(args.steps):
+            window((args.warmup + k) * W)
+        t1.record(stream)
+        timed_region_edge(world)
+    dev_ms = t0.elapsed_time(t1)
+    # end to end: the window's snapshots host -> device, run + drain, device -> host
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    out_pin = torch.empty(W * eff, dtype=torch.int32).pin_memory()
+    timed_region_edge(world)
+    e0.record(stream)
+    for k in range(args.steps):
+        c0 = (args.warmup + k) * W
+        st[c0 * eff:(c0 + W + 1) * eff].copy_(host_pin[c0 * eff:(c0 + W + 1) * eff], non_blocking=True)
+        window(c0)
+        out_pin.copy_(st[(c0 + 1) * eff:(c0 + W + 1) * eff], non_blocking=True)
+    e1.record(stream)
+    timed_region_edge(world)
+    e2e_ms = e0.elapsed_time(e1)
+    script_b, state_b = algorithmic_bytes_per_cycle(s, arrivals=True)
+    return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=1, clocks=ck.summary(),
+                bytes_per_cycle=script_b + state_b, kernel_ms=dev_ms / args.steps,
+                h2d=(W + 1) * eff * 4, d2h=W * eff * 4, launches_per_step=2,
+                design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
+                            script_mb_per_cycle=script_b / 1e6, rio=rio,
+                            major_stages=s.num_major_stages, blocks=nb,
+                            setup_violations=stats["setup_violations"],
+                            hold_violations=stats["hold_violations"],
+                            events_dropped=stats["events_dropped"]),
+                script=s, d=d)
+
+
+def multi_design_sizes(n=12, lo=50_000, hi=4_000_000, seed=4):
+    """AND-node counts log-uniform in [lo, hi] (seeded)."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size=n)).astype(np.int64)
+
+
+def run_mine_multi(args, rank, world):
+    """Twelve designs of log-uniform size in [50k, 4M] AND nodes in one
+    persistent launch (scripts relocated into one), replayed from a CUDA
+    graph; 8 lane words (256 streams) per design."""
+    import torch
+    from jacquard_b200 import batched
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    sizes = multi_design_sizes()
+    scripts, ands = [], 0
+    for k, n_and in enumerate(sizes.tolist()):
+        clusters = max(1, int(round(n_and / 4096)))
+        d = build_design(seed=40 + 100 * rank + k, clusters=clusters,
+                         n_dff=max(64, 200_000 * clusters // 512))
+        ands += int(d.num_and)
+        scripts.append(build_script(d, 148))
+    comb = batched.CombinedScript(scripts)
+    lanes = args.lanes
+    B = batched.BatchedSim(comb, lanes, device=dev)
+    B.load_state(np.zeros((lanes, B.sig), np.uint32))
+    B.reset_sram(x=True)
+    W = args.window
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):
+        B.run(None, W, stream=stream)
+        stream.synchronize()
+        assert B.status(stream) == 0
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            B.run(None, W, stream=stream)
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    assert B.status(stream) == 0
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as ck:
+        timed_region_edge(world)
+        t0.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(args.steps):
+                g.replay()
+        t1.record(stream)
+        timed_region_edge(world)
+    dev_ms = t0.elapsed_time(t1)
+    assert B.status(stream) == 0
+    streams = 32 * lanes * len(scripts)
+    per = [algorithmic_bytes_per_cycle(s) for s in scripts]
+    bytes_per_cycle = sum(p[0] for p in per) + 32 * lanes * sum(p[1] for p in per)
+    return dict(dev_ms=dev_ms, e2e_ms=None, cycles_per_step=W, streams=streams,
+                clocks=ck.summary(), bytes_per_cycle=bytes_per_cycle, kernel_ms=dev_ms / args.steps,
+                h2d=0, d2h=0, launches_per_step=2,
+                design=dict(designs=len(scripts), ands=ands, sizes=sizes.tolist(),
+                            partitions=int(sum(s.num_partitions for s in scripts)),
+                            script_mb_per_cycle=comb.script_words_per_cycle() * 4 / 1e6,
+                            lanes=lanes, graph=True),
+                script=None, d=None)
+
+
 def compare_kernels(d, args, window=16, reps=3):
     """Single-stream cycles/s of the plain interpreter (reference state layout,
     one stimulus stream) on a script of the same design, built for 296
@@ -408,7 +567,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--mode", default="batched", choices=["plain", "batched"])
+    ap.add_argument("--mode", default="batched", choices=["plain", "batched", "timed", "multi"],
+                    help="batched: 256 streams (default); plain: 1 stream; timed: arrivals + "
+                         "setup/hold checks with event drain; multi: 12 designs in one graph-captured launch")
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
     ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
@@ -444,7 +605,7 @@ def main():
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * args.cpu_cycles / v, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-                "config": {"workload": "soc-2M: 2^21 clustered ANDs + reset gates, depth 80, 200k DFF, 16 SRAM 1024x32, X-prop",
+                "config": {"workload": SOC,
                            "sample": f"{args.cpu_cycles} cycles per step, 1 stimulus stream"},
                 "cpu_baseline": {"value": v, "unit": "stimulus-cycles/s", "cores": threads,
                                  "kind": "port",
@@ -459,24 +620,30 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    r = run_mine_batched(args, rank, world) if args.mode == "batched" else run_mine_plain(args, rank, world)
+    runner = {"batched": run_mine_batched, "plain": run_mine_plain, "timed": run_mine_timed,
+              "multi": run_mine_multi}[args.mode]
+    r = runner(args, rank, world)
     total_cycles = r["cycles_per_step"] * r["streams"] * args.steps
-    mine_val, e2e_val, dev_ms, _ = replica_throughput(total_cycles, r["dev_ms"], r["e2e_ms"], world)
+    mine_val, e2e_val, dev_ms, _ = replica_throughput(total_cycles, r["dev_ms"],
+                                                      r["e2e_ms"] or r["dev_ms"], world)
+    if r["e2e_ms"] is None:
+        e2e_val = None  # no host-buffer path measured in this mode
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
     if rank == 0:
         peak, peak_kind = peaks()
         achieved = r["bytes_per_cycle"] * r["cycles_per_step"] / (r["kernel_ms"] / 1e3) / 1e9
-        if args.no_cpu:
+        if args.no_cpu or args.mode in ("timed", "multi"):
             cpu_v, cpu_dt = None, 0.0
         else:
             cpu_v, cpu_dt = cpu_baseline(r["script"], r["d"], cycles=args.cpu_cycles, threads=1)
+        workload = WORKLOADS[args.mode]
         line = {"metric": METRIC, "value": mine_val, "unit": "stimulus-cycles/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-                "config": {"workload": "soc-2M: 2^21 clustered ANDs + reset gates, depth 80, 200k DFF, 16 SRAM 1024x32, X-prop",
+                "config": {"workload": workload,
                            "mode": args.mode, "streams": r["streams"],
                            "cycles_per_step": r["cycles_per_step"], "l2": "inputs larger than L2 (snapshot window + script)",
                            **r["design"]},
@@ -488,8 +655,9 @@ def main():
                 "cpu_baseline": {"value": cpu_v, "unit": "stimulus-cycles/s", "cores": 1,
                                  "kind": "port",
                                  "sample": f"{args.cpu_cycles} cycles x 1 stream, {cpu_dt:.1f} s"},
-                "e2e": {"value": e2e_val, "unit": "stimulus-cycles/s",
-                        "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+                "e2e": ({"value": e2e_val, "unit": "stimulus-cycles/s",
+                         "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]}
+                        if e2e_val is not None else None),
                 "gpu_launches": r["launches_per_step"] * args.steps,
                 "clocks": r["clocks"]}
         if args.compare and args.mode == "batched":
