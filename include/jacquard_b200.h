@@ -116,7 +116,11 @@ int jq_max_blocks(int device, size_t *max_blocks);
  * streams 32l..32l+31.  Two snapshot buffers ping-pong: cycle c reads state_a when c
  * is even (state_b when odd) and writes the other; after num_cycles cycles the
  * final state is in state_a if num_cycles is even, else state_b.  Both buffers
- * must start with snapshot 0 (values, X template).  No timing checks. */
+ * must start with snapshot 0 (values, X template).  Words that no partition
+ * writes (inputs aside, which come from `stimulus`) keep their snapshot-0
+ * value in every cycle, where the plain interpreter keeps each snapshot's
+ * host pre-fill; the two agree when every snapshot carries the same pre-fill
+ * (the X template).  No timing checks. */
 typedef struct {
   size_t num_blocks, num_major_stages;
   const size_t *blocks_start;  /* device */
@@ -257,6 +261,16 @@ int jq_output_transitions(const uint32_t *states, size_t first_snapshot, size_t 
                           const uint32_t *out_pos, const uint32_t *out_const, uint32_t n_out,
                           uint32_t *counts, unsigned long long *offsets, uint32_t *transitions,
                           uint32_t *arrivals, size_t capacity, size_t *total, void *stream);
+
+/* Set bits for the display / assertion post-scan (no counterpart in the
+ * reference, whose post-scan probes every condition of every snapshot on the
+ * host, src/bin/jacquard.rs:1152-1253).  Same walk and outputs as
+ * jq_output_transitions.  Each entry j | 1 << 30 is a condition bit
+ * bit_pos[j] that is 1 in that snapshot. */
+int jq_set_bits(const uint32_t *states, size_t first_snapshot, size_t num_snapshots,
+                size_t snapshot_words, const uint32_t *bit_pos, uint32_t n_bits, uint32_t *counts,
+                unsigned long long *offsets, uint32_t *hits, size_t capacity, size_t *total,
+                void *stream);
 
 /* Human-readable text for a status code. */
 const char *jq_strerror(int code);

@@ -41,6 +41,23 @@ typedef struct {
 
 void *jqf_generate(const jqf_gen_params *p, uint64_t *num_and);
 void jqf_free_design(void *design);
+
+/* AIG builder for designs read from a gate-level netlist (the handle is a
+ * design: free it with jqf_free_design).  Signals are "iv" = pin << 1 |
+ * invert; pin 0 is constant 0, so iv 0 / 1 are the constants.  Sources can
+ * be added at any time.  jqf_builder_and folds constants and reuses an
+ * existing gate for the same fanins (src/aig.rs:327-345), and returns the
+ * gate's iv.  jqf_builder_output appends a primary output (unique) and
+ * returns its index.  jqf_builder_finish checks the design and records its
+ * clock-flag / reset pins for the stimulus helpers. */
+void *jqf_builder_new(void);
+uint32_t jqf_builder_input(void *b);
+uint32_t jqf_builder_clock_flag(void *b);
+uint32_t jqf_builder_dff(void *b);
+int jqf_builder_set_dff(void *b, uint32_t index, uint32_t d_iv, uint32_t en_iv);
+uint32_t jqf_builder_and(void *b, uint32_t a_iv, uint32_t b_iv);
+int64_t jqf_builder_output(void *b, uint32_t iv);
+int jqf_builder_finish(void *b, uint32_t clock_flag_pin, uint32_t reset_pin);
 int jqf_design_info(void *design, jqf_design_info_t *out);
 /* Copy one design array (see capi.cpp for `which`); returns its byte size. */
 int64_t jqf_design_array(void *design, int which, void *dst, size_t cap);

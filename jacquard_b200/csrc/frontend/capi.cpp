@@ -13,6 +13,7 @@ namespace {
 struct Design {
   AIG g;
   GenInfo info;
+  uint32_t n_inputs = 0;  // input pins added by the builder
 };
 CostModel unpack_model(const float *m) {
   CostModel cm;
@@ -73,6 +74,72 @@ void *jqf_generate(const jqf_gen_params *p, uint64_t *num_and) {
 }
 
 void jqf_free_design(void *d) { delete static_cast<Design *>(d); }
+
+// ---- AIG builder for designs read from a gate-level netlist.  Sources
+// (inputs, clock flags, DFF Q pins) can be added at any time; AND gates are
+// structurally hashed and constant-folded (src/aig.rs:327-345), so pins stay
+// in topological order.
+void *jqf_builder_new(void) {
+  try {
+    return new Design;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+uint32_t jqf_builder_input(void *b) {
+  auto *d = static_cast<Design *>(b);
+  return d->g.add_pin(DRV_INPUT, d->n_inputs++);
+}
+
+uint32_t jqf_builder_clock_flag(void *b) {
+  return static_cast<Design *>(b)->g.add_pin(DRV_CLKFLAG, 0);
+}
+
+uint32_t jqf_builder_dff(void *b) {
+  auto *d = static_cast<Design *>(b);
+  uint32_t i = (uint32_t)d->g.dffs.size();
+  d->g.dffs.emplace_back();
+  d->g.dffs[i].q = d->g.add_pin(DRV_DFF, i);
+  return d->g.dffs[i].q;
+}
+
+int jqf_builder_set_dff(void *b, uint32_t index, uint32_t d_iv, uint32_t en_iv) {
+  auto *d = static_cast<Design *>(b);
+  if (index >= d->g.dffs.size() || (d_iv >> 1) > d->g.num_pins || (en_iv >> 1) > d->g.num_pins)
+    return -1;
+  d->g.dffs[index].d_iv = d_iv;
+  d->g.dffs[index].en_iv = en_iv;
+  return 0;
+}
+
+uint32_t jqf_builder_and(void *b, uint32_t a_iv, uint32_t b_iv) {
+  auto *d = static_cast<Design *>(b);
+  if ((a_iv >> 1) > d->g.num_pins || (b_iv >> 1) > d->g.num_pins) return NONE;
+  const uint32_t before = d->g.num_pins;
+  const uint32_t r = d->g.add_and(a_iv, b_iv);
+  d->info.num_and += d->g.num_pins - before;
+  return r;
+}
+
+int64_t jqf_builder_output(void *b, uint32_t iv) {
+  auto *d = static_cast<Design *>(b);
+  if ((iv >> 1) > d->g.num_pins) return -1;
+  auto &po = d->g.primary_outputs;
+  for (size_t i = 0; i < po.size(); ++i)
+    if (po[i] == iv) return (int64_t)i;
+  po.push_back(iv);
+  return (int64_t)po.size() - 1;
+}
+
+int jqf_builder_finish(void *b, uint32_t clock_flag_pin, uint32_t reset_pin) {
+  auto *d = static_cast<Design *>(b);
+  for (const DFF &f : d->g.dffs)
+    if (f.q == 0) return -1;
+  d->info.clock_flag_pin = clock_flag_pin;
+  d->info.reset_pin = reset_pin;
+  return 0;
+}
 
 int jqf_design_info(void *dp, jqf_design_info_t *out) {
   auto *d = static_cast<Design *>(dp);

@@ -1,10 +1,12 @@
-// Output-signal transitions of a simulation run, for the waveform writers
-// (src/sim/vcd_io.rs:758-946 walk every output of every snapshot on the host
-// and keep the ones whose value changed).  Here the walk runs on the device
-// over the resident snapshots: each snapshot's outputs are encoded
-// (0, 1, or 3 for X), compared with the previous snapshot's code (2 before
-// the first), and the changes are compacted in (snapshot, output) order, so
-// the host only formats the transitions.
+// Per-snapshot walks over the resident snapshots of a run, compacted on the
+// device in (snapshot, signal) order, so the host only formats results:
+// - output transitions for the waveform writers (src/sim/vcd_io.rs:758-946
+//   walk every output of every snapshot on the host and keep the changes):
+//   each output is encoded (0, 1, or 3 for X) and compared with the previous
+//   snapshot's code (2 before the first);
+// - set bits for the display / assertion post-scan
+//   (src/bin/jacquard.rs:1152-1253 probe every condition bit of every
+//   snapshot on the host): a condition fires where its bit is 1.
 #include "sim_common.cuh"
 
 namespace jqk {
@@ -19,6 +21,7 @@ struct TransParams {
   const uint32_t *out_pos;  // state bit position of each output, or ~0u for a constant
   const uint32_t *out_const;  // value of constant outputs (may be null: 0)
   uint32_t n_out;
+  int set_bits;               // 1: report set bits instead of transitions
 };
 
 __device__ __forceinline__ uint32_t out_code(const TransParams &P, size_t s, uint32_t j) {
@@ -33,6 +36,7 @@ __device__ __forceinline__ uint32_t out_code(const TransParams &P, size_t s, uin
 
 __device__ __forceinline__ bool changed(const TransParams &P, size_t s, uint32_t j, uint32_t &code) {
   code = out_code(P, s, j);
+  if (P.set_bits) return code == 1u;
   const uint32_t prev = s == 0 ? 2u : out_code(P, s - 1, j);
   return code != prev;
 }
@@ -115,6 +119,28 @@ __global__ void __launch_bounds__(OT) trans_write_kernel(TransParams P,
 
 using namespace jqk;
 
+static int run_walk(TransParams P, uint32_t *counts, unsigned long long *offsets,
+                    uint32_t *transitions, uint32_t *arrivals, size_t capacity, size_t *total,
+                    void *stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  *total = 0;
+  if (P.num == 0) return JQ_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)(P.num < (size_t)sms * 8 ? P.num : (size_t)sms * 8);
+  trans_count_kernel<<<grid, OT, 0, st>>>(P, counts);
+  trans_scan_kernel<<<1, OT, 0, st>>>(counts, P.num, offsets);
+  if (capacity) trans_write_kernel<<<grid, OT, 0, st>>>(P, offsets, transitions, arrivals, capacity);
+  if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
+  unsigned long long t = 0;
+  if (cudaMemcpyAsync(&t, offsets + P.num, sizeof(t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return JQ_ERR_CUDA;
+  *total = (size_t)t;
+  return t > capacity ? JQ_ERR_EVENT_OVERFLOW : JQ_OK;
+}
+
 extern "C" int jq_output_transitions(const uint32_t *states, size_t first_snapshot,
                                      size_t num_snapshots, size_t snapshot_words,
                                      size_t xmask_offset, size_t arrival_offset,
@@ -126,24 +152,19 @@ extern "C" int jq_output_transitions(const uint32_t *states, size_t first_snapsh
   if (!states || !out_pos || !counts || !offsets || !total || snapshot_words == 0 || n_out == 0 ||
       n_out >= (1u << 30) || (capacity && !transitions))
     return JQ_ERR_INVALID_ARG;
-  cudaStream_t st = (cudaStream_t)stream;
-  *total = 0;
-  if (num_snapshots == 0) return JQ_OK;
   TransParams P{states, first_snapshot, num_snapshots, snapshot_words, xmask_offset,
-                arrival_offset, out_pos, out_const, n_out};
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned grid = (unsigned)(num_snapshots < (size_t)sms * 8 ? num_snapshots : (size_t)sms * 8);
-  trans_count_kernel<<<grid, OT, 0, st>>>(P, counts);
-  trans_scan_kernel<<<1, OT, 0, st>>>(counts, num_snapshots, offsets);
-  if (capacity) trans_write_kernel<<<grid, OT, 0, st>>>(P, offsets, transitions, arrivals, capacity);
-  if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
-  unsigned long long t = 0;
-  if (cudaMemcpyAsync(&t, offsets + num_snapshots, sizeof(t), cudaMemcpyDeviceToHost, st) !=
-          cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return JQ_ERR_CUDA;
-  *total = (size_t)t;
-  return t > capacity ? JQ_ERR_EVENT_OVERFLOW : JQ_OK;
+                arrival_offset, out_pos, out_const, n_out, 0};
+  return run_walk(P, counts, offsets, transitions, arrivals, capacity, total, stream);
+}
+
+extern "C" int jq_set_bits(const uint32_t *states, size_t first_snapshot, size_t num_snapshots,
+                           size_t snapshot_words, const uint32_t *bit_pos, uint32_t n_bits,
+                           uint32_t *counts, unsigned long long *offsets, uint32_t *hits,
+                           size_t capacity, size_t *total, void *stream) {
+  if (!states || !bit_pos || !counts || !offsets || !total || snapshot_words == 0 || n_bits == 0 ||
+      n_bits >= (1u << 30) || (capacity && !hits))
+    return JQ_ERR_INVALID_ARG;
+  TransParams P{states, first_snapshot, num_snapshots, snapshot_words, 0, 0, bit_pos, nullptr,
+                n_bits, 1};
+  return run_walk(P, counts, offsets, hits, nullptr, capacity, total, stream);
 }

@@ -69,6 +69,19 @@ def _lib():
         vp, sz, u32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32
         lib.jqf_validate.restype = ctypes.c_int
         lib.jqf_validate.argtypes = [vp, sz, sz, vp, sz, u32, u32, sz, ctypes.c_char_p, sz]
+        lib.jqf_builder_new.restype = vp
+        lib.jqf_builder_new.argtypes = []
+        for fn in ("jqf_builder_input", "jqf_builder_clock_flag", "jqf_builder_dff"):
+            getattr(lib, fn).restype = u32
+            getattr(lib, fn).argtypes = [vp]
+        lib.jqf_builder_set_dff.restype = ctypes.c_int
+        lib.jqf_builder_set_dff.argtypes = [vp, u32, u32, u32]
+        lib.jqf_builder_and.restype = u32
+        lib.jqf_builder_and.argtypes = [vp, u32, u32]
+        lib.jqf_builder_output.restype = ctypes.c_int64
+        lib.jqf_builder_output.argtypes = [vp, u32]
+        lib.jqf_builder_finish.restype = ctypes.c_int
+        lib.jqf_builder_finish.argtypes = [vp, u32, u32]
         lib.jqf_constraint_buffer.restype = ctypes.c_int
         lib.jqf_constraint_buffer.argtypes = [u32, ctypes.c_uint64, sz, vp, vp, vp, vp,
                                               ctypes.POINTER(u32), vp]
@@ -125,6 +138,20 @@ class Design:
         self._h = lib.jqf_generate(ctypes.byref(gp), ctypes.byref(n_and))
         if not self._h:
             raise RuntimeError("design generation failed")
+        self._load_info()
+
+    @classmethod
+    def from_handle(cls, handle):
+        """A design built elsewhere (e.g. by the netlist reader through the
+        jqf_builder_* entry points); takes ownership of the handle."""
+        d = cls.__new__(cls)
+        d.params = None
+        d._h = handle
+        d._load_info()
+        return d
+
+    def _load_info(self):
+        lib = _lib()
         info = _DesignInfo()
         lib.jqf_design_info(self._h, ctypes.byref(info))
         self.num_pins = info.num_pins

@@ -13,8 +13,11 @@ Restates the reference's host-side VCD path (src/sim/vcd_io.rs):
 
 The reference reads and writes VCD with the vcd-ng crate (0.2.0, not present
 here).  This module has its own reader and writer for the VCD grammar of IEEE
-1364 section 18.  A vector value shorter than its variable is left-extended
-as that grammar specifies.
+1364 section 18.  A vector value is used exactly as written.  Its i-th
+character goes to bit position i of the variable (most significant first),
+and a value shorter than the variable is not extended.  That is how
+parse_input_vcd consumes vcd-ng's tokens, and the reference's own fixtures
+depend on it: tests/assert_test feeds "b11" to a 4-bit input.
 
 For long runs, `device_transitions` does the per-snapshot output walk on the
 GPU (`jq_output_transitions`), and the writers only format the changes.
@@ -64,7 +67,6 @@ class VcdReader:
         self.timescale = None
         self.scopes = []
         self._pos = 0
-        self._sizes = {}
         self._read_header()
 
     def _until_end(self):
@@ -107,7 +109,6 @@ class VcdReader:
                     ref, idx = ref.split("[", 1)
                     index = _parse_index("[" + idx)
                 v = Var(kind, size, code, ref, index)
-                self._sizes[code] = size
                 (stack[-1].children if stack else self.scopes).append(v)
             elif kw.startswith("$"):
                 self._until_end()
@@ -125,14 +126,10 @@ class VcdReader:
             elif c in "01xXzZ":
                 yield ("v", tok[1:], tok[0].lower())
             elif c in "bB":
-                bits = tok[1:].lower()
-                code = w[i]
+                # the characters as written, not extended to the variable's
+                # width: a short value sets only its leading positions
+                yield ("v", w[i], tok[1:].lower())
                 i += 1
-                size = self._sizes.get(code, len(bits))
-                if len(bits) < size:
-                    pad = bits[0] if bits[0] in "xz" else "0"
-                    bits = pad * (size - len(bits)) + bits
-                yield ("v", code, bits)
             elif c in "rR":
                 i += 1  # real values are not input stimulus
             elif tok in ("$dumpvars", "$dumpall", "$dumpon", "$dumpoff", "$end"):
@@ -312,7 +309,7 @@ class VcdWriter:
         self._buf = []
 
     def timescale(self, ratio, unit):
-        self.f.write(f"$timescale {ratio}{unit} $end\n")
+        self.f.write(f"$timescale {ratio} {unit} $end\n")
 
     def add_module(self, name):
         self.f.write(f"$scope module {name} $end\n")
@@ -572,21 +569,23 @@ def write_stimulus_vcd(f, ports, in_vals, input_layout, clock_flag_pin, period=1
     w.flush()
 
 
-def simulate_vcd(script, design, stimulus_text, xprop_all_x=False, device="cuda", stream=None):
+def simulate_vcd(script, ports, stimulus_text, xprop_all_x=False, device="cuda", stream=None):
     """The reference's VCD-in / VCD-out flow on the plain interpreter: parse
     the stimulus, expand the snapshots (X template when the script has X
     propagation; every DFF/SRAM bit X at start with xprop_all_x), run all
     cycles on the device, and write the output waveform from the device-side
-    transition walk.  Returns (output VCD text, device states)."""
+    transition walk.  `ports` maps VCD variables to the design (DesignPorts
+    for generated designs, netlist.NetlistPorts for netlists).  Returns
+    (output VCD text, device states)."""
     import io as _io
 
     import torch
     from . import sim, state as st
-    ports = DesignPorts(design, script)
     reader = VcdReader(stimulus_text)
-    found = auto_detect_vcd_scope(reader.scopes, ["clk"])
+    required = sorted({name for name, _ in ports.input_pins})
+    found = auto_detect_vcd_scope(reader.scopes, required)
     if found is None:
-        raise ValueError("no scope with a clk input in the stimulus")
+        raise ValueError("no scope holds every input port of the design")
     vcd2inp = match_vcd_inputs(found[1], ports.input_pins)
     snaps, ots = parse_input_vcd(reader, vcd2inp, ports.input_pos, ports.clock_pins,
                                  script.reg_io_state_size)

@@ -72,7 +72,7 @@ def test_vcd_in_simulate_vcd_out_matches_oracle(kind, nb, split, xprop):
     buf = io.StringIO()
     vcd.write_stimulus_vcd(buf, ports, vals, s.input_layout, d.clock_flag_pin, period=10)
     text = buf.getvalue()
-    got_text, dev_states = vcd.simulate_vcd(s, d, text, xprop_all_x=xprop)
+    got_text, dev_states = vcd.simulate_vcd(s, ports, text, xprop_all_x=xprop)
 
     # the same flow with the oracle and the reference writer's host walk
     r = vcd.VcdReader(text)
@@ -106,3 +106,43 @@ def test_vcd_in_simulate_vcd_out_matches_oracle(kind, nb, split, xprop):
     vcd.write_output_vcd(w, out2vcd, ots, values, xmask)
     assert got_text == out.getvalue()
     assert sum(line.startswith("#") for line in got_text.splitlines()) == len(ots) - 1
+
+
+@pytest.mark.parametrize("gv,stim,want", [("dff_test_synth.gv", "dff_test.vcd", "dff_test_output.vcd"),
+                                          ("assert_synth.gv", "assert_test.vcd", "assert_test_output.vcd")])
+def test_reference_fixtures_on_the_gpu(gv, stim, want):
+    """The reference's netlist + stimulus fixtures through the plain
+    interpreter and the device transition walk: the reference's output VCD."""
+    import test_netlist_golden as golden
+    from jacquard_b200 import netlist, observe
+    nd = netlist.read_netlist(golden.read(gv))
+    s = nd.design.build_script(num_blocks=1)
+    ports = netlist.NetlistPorts(nd, s)
+    text, dev = vcd.simulate_vcd(s, ports, golden.read(stim))
+    assert text.strip() == golden.read(want).strip()
+    # assertion post-scan: device probe == host probe over the same snapshots
+    rio = s.reg_io_state_size
+    cycles = dev.numel() // rio - 1
+    host = sim.dev_to_u32(dev)
+    asserts = ports.assertion_positions(s)
+    if asserts:
+        assert observe.device_post_scan(dev, cycles, rio, assertions=asserts) == \
+            observe.post_scan(host, cycles, rio, assertions=asserts)
+
+
+def test_display_post_scan_on_the_gpu():
+    import os
+    import test_observe
+    from jacquard_b200 import netlist, observe
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "display_counter.gv")) as f:
+        nd = netlist.read_netlist(f.read())
+    s = nd.design.build_script(num_blocks=1)
+    ports = netlist.NetlistPorts(nd, s)
+    _, dev = vcd.simulate_vcd(s, ports, test_observe.stimulus(30))
+    rio = s.reg_io_state_size
+    cycles = dev.numel() // rio - 1
+    disp = ports.display_positions(s)
+    got = observe.device_post_scan(dev, cycles, rio, displays=disp)
+    want = observe.post_scan(sim.dev_to_u32(dev), cycles, rio, displays=disp)
+    assert got == want and len(got[0]) >= 5

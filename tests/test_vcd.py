@@ -106,8 +106,8 @@ b1 #
     assert m[('"', 0)] == "d3" and m[('"', 3)] == "d0"
     assert m[("#", 0)] == "s2" and m[("#", 2)] == "s0"
     toks = list(r.tokens())
-    # short vector values are left-extended with 0
-    assert ("v", '"', "0101") in toks and ("v", "#", "001") in toks
+    # vector values are used as written (no extension to the variable width)
+    assert ("v", '"', "101") in toks and ("v", "#", "1") in toks
 
 
 @pytest.mark.parametrize("kind,nb,split", [("tiny", 8, (5,)), ("sram", 16, (8,))])
