@@ -272,6 +272,35 @@ int jq_set_bits(const uint32_t *states, size_t first_snapshot, size_t num_snapsh
                 unsigned long long *offsets, uint32_t *hits, size_t capacity, size_t *total,
                 void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* RepCut hypergraph build (src/repcut.rs:58-176) on the device, from the
+ * arrays of jqf_repcut_slice and the design arrays (kind, fa, fb).  All
+ * pointers are device memory except the two level-start arrays, which the
+ * host walks to launch one pass per level:
+ *   rlevel_nodes: pins 1..num_pins ordered by reverse level,
+ *     rlevel_start_host[num_rlevels+1];
+ *   flevel_nodes: likewise by forward level;
+ *   nfe[pin]: number of endpoint-input occurrences of the pin;
+ *   supp_start_host / supp_edges / wsupp: the traversal-order exceptions of
+ *     jqf_repcut_slice;
+ *   sets, cone, supp_bits: workspace of (num_pins+1) * 64 u64,
+ *     (num_pins+1) bytes and num_fanouts / 32 + 2 words.
+ * Outputs per pin: fingerprint[2*(num_pins+1)] (equal endpoint sets give
+ * equal fingerprints), popcount (endpoints reached), node_weight (f32, 0
+ * outside the cone); endpoint_weight[num_endpoints].  Asynchronous on
+ * `stream`. */
+int jq_repcut_build(uint32_t num_pins, const uint8_t *kind, const uint32_t *fa, const uint32_t *fb,
+                    const uint32_t *fanout_start, const uint32_t *fanouts, const uint8_t *staged,
+                    uint32_t num_endpoints, const uint32_t *ep_start, const uint32_t *ep_pins,
+                    const uint32_t *nfe, const uint32_t *rlevel_nodes,
+                    const uint32_t *rlevel_start_host, uint32_t num_rlevels,
+                    const uint32_t *flevel_nodes, const uint32_t *flevel_start_host,
+                    uint32_t num_flevels, const uint32_t *supp_start_host,
+                    const uint32_t *supp_edges, const uint8_t *wsupp, uint32_t num_fanouts,
+                    uint32_t *supp_bits, unsigned long long *sets, uint8_t *cone,
+                    unsigned long long *fingerprint, uint32_t *popcount, float *node_weight,
+                    unsigned long long *endpoint_weight, void *stream);
+
 /* Human-readable text for a status code. */
 const char *jq_strerror(int code);
 

@@ -103,6 +103,25 @@ int jqf_script_features(void *design, void *script, float *out);
 /* Host inference of a cost model on `n` feature rows (log kernel cycles). */
 int jqf_cost_model_predict(const float *model, const float *features, size_t n, float *out);
 
+/* RepCut hypergraph inputs of staged slice `slice` of the design under the
+ * given level split (src/repcut.rs:58-176).  Outputs:
+ *   - the fanout CSR of the AIG and the endpoint-group input pins (CSR);
+ *   - staged-input flags;
+ *   - the reverse / forward levels that schedule the propagation;
+ *   - the traversal-order exceptions of the reference: per block of 4096
+ *     endpoints the fanout edges that do not propagate (supp_start /
+ *     supp_edges), and per-pin fanin weights that are skipped (wsupp).
+ * Arrays may be NULL, which returns sizes only:
+ *   fanout_start[num_pins+2], ep_start[E+1], supp_start[blocks+1];
+ *   staged / rlevel / flevel / wsupp [num_pins+1];
+ *   sizes = {E, fanouts length, ep_pins length, supp_edges length}.
+ * Returns the number of slices, or -1. */
+int jqf_repcut_slice(void *design, const uint32_t *level_split, size_t n_split, uint32_t slice,
+                     uint32_t *fanout_start, uint32_t *fanouts, uint32_t *ep_start,
+                     uint32_t *ep_pins, uint8_t *staged, uint32_t *rlevel, uint32_t *flevel,
+                     uint32_t *supp_start, uint32_t *supp_edges, uint8_t *wsupp,
+                     uint64_t *sizes);
+
 /* Host-side script validator (same walk as the kernel). 0 = valid. */
 int jqf_validate(const uint64_t *blocks_start, size_t num_blocks, size_t num_major_stages,
                  const uint32_t *blocks_data, size_t blocks_data_len,

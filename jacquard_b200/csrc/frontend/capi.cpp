@@ -5,6 +5,8 @@
 #include <stdexcept>
 
 #include "frontend.hpp"
+
+#include <algorithm>
 #include "../../../include/jacquard_frontend.h"
 
 using namespace jq;
@@ -305,6 +307,154 @@ int64_t jqf_script_array(void *sp, int which, void *dst, size_t cap) {
   if (!src) { src = tmp.data(); bytes = tmp.size() * 4; }
   if (dst && cap >= bytes) std::memcpy(dst, src, bytes);
   return (int64_t)bytes;
+}
+
+// ---- RepCut hypergraph inputs of one staged slice (src/repcut.rs:58-176).
+// Fills (each pointer may be null to only get sizes):
+//   fanout_start[num_pins + 2], fanouts[]: AND-gate fanouts of every pin,
+//     built as src/aig.rs:2640-2669 does (counts, prefix sums, filled from
+//     the back in driver order);
+//   ep_start[E + 1], ep_pins[]: each endpoint group's input pins
+//     (EndpointGroup::for_each_input order, duplicates kept);
+//   staged[num_pins + 1]: 1 for the slice's staged inputs (traversal stops);
+//   rlevel[num_pins + 1]: 0 for pins without AND fanouts, else 1 + the
+//     largest rlevel of a fanout;
+//   flevel[num_pins + 1]: 0 for non-AND pins, else 1 + the largest flevel
+//     of the AND fanins.
+// sizes[0] = number of endpoint groups E, sizes[1] = fanout list length,
+// sizes[2] = ep_pins length.
+// The reference's results depend on its traversal order (TopoTraverser,
+// src/aig.rs:3125-3170) where a staged input and one of its fanins are both
+// in a cone.  The traversal is restated to report those cases:
+//   supp_start[blocks + 1], supp_edges[]: per block of 4096 endpoints, the
+//     fanout-edge indices k (fanouts[k] = staged j, k in i's range) along
+//     which i, coming later in the block's post-order, does not take j's set;
+//   wsupp[num_pins + 1]: bit 0 / bit 1 when a staged pin comes before its
+//     fanin a / b in the all-endpoint post-order, so its weight misses that
+//     fanin's.
+// sizes[3] = supp_edges length.
+static uint32_t repcut_topo(const AIG &g, const std::vector<uint8_t> &stg, const uint32_t *starts,
+                            size_t n_start, std::vector<int32_t> &pos,
+                            std::vector<uint32_t> &touched) {
+  std::vector<uint32_t> stack;
+  stack.reserve(n_start + 64);
+  for (size_t k = 0; k < n_start; ++k) stack.push_back(starts[k] << 1);
+  uint32_t n = 0;
+  while (!stack.empty()) {
+    const uint32_t item = stack.back();
+    stack.pop_back();
+    const uint32_t u = item >> 1;
+    if (item & 1) {
+      pos[u] = (int32_t)n++;
+      continue;
+    }
+    if (pos[u] != -1) continue;
+    pos[u] = -2;  // visited, not yet post-ordered
+    touched.push_back(u);
+    stack.push_back((u << 1) | 1);
+    if (g.kind[u] == DRV_AND && !stg[u]) {
+      if (g.fb[u] >> 1) stack.push_back((g.fb[u] >> 1) << 1);
+      if (g.fa[u] >> 1) stack.push_back((g.fa[u] >> 1) << 1);
+    }
+  }
+  return n;
+}
+
+int jqf_repcut_slice(void *dp, const uint32_t *level_split, size_t n_split, uint32_t slice,
+                     uint32_t *fanout_start, uint32_t *fanouts, uint32_t *ep_start,
+                     uint32_t *ep_pins, uint8_t *staged, uint32_t *rlevel, uint32_t *flevel,
+                     uint32_t *supp_start, uint32_t *supp_edges, uint8_t *wsupp,
+                     uint64_t *sizes) {
+  try {
+    auto *d = static_cast<Design *>(dp);
+    const AIG &g = d->g;
+    std::vector<uint32_t> split(level_split, level_split + n_split);
+    std::vector<StagedAIG> st = build_staged_aigs(g, split);
+    if (slice >= st.size()) return -1;
+    const StagedAIG &sa = st[slice];
+    const uint32_t N = g.num_pins;
+    std::vector<uint32_t> fs(N + 2, 0);
+    for (uint32_t p = 1; p <= N; ++p)
+      if (g.kind[p] == DRV_AND) {
+        if (g.fa[p] >> 1) fs[g.fa[p] >> 1]++;
+        if (g.fb[p] >> 1) fs[g.fb[p] >> 1]++;
+      }
+    for (uint32_t i = 1; i < N + 2; ++i) fs[i] += fs[i - 1];
+    std::vector<uint32_t> fo(fs[N + 1]);
+    for (uint32_t p = 0; p <= N; ++p)
+      if (g.kind[p] == DRV_AND) {
+        if (g.fa[p] >> 1) fo[--fs[g.fa[p] >> 1]] = p;
+        if (g.fb[p] >> 1) fo[--fs[g.fb[p] >> 1]] = p;
+      }
+    const size_t E = sa.num_endpoint_groups();
+    std::vector<uint32_t> es(E + 1, 0), ep;
+    for (size_t e = 0; e < E; ++e) {
+      sa.for_each_input(g, e, [&](uint32_t pin) { ep.push_back(pin); });
+      es[e + 1] = (uint32_t)ep.size();
+    }
+    auto is_staged = [&](uint32_t p) { return sa.has_staged_inputs && sa.is_staged_input[p]; };
+    std::vector<uint32_t> rl(N + 1, 0), fl(N + 1, 0);
+    for (uint32_t p = N; p >= 1; --p) {
+      uint32_t m = 0;
+      bool any = false;
+      for (uint32_t k = fs[p]; k < fs[p + 1]; ++k) {
+        any = true;
+        m = std::max(m, rl[fo[k]]);
+      }
+      rl[p] = any ? m + 1 : 0;
+    }
+    for (uint32_t p = 1; p <= N; ++p)
+      if (g.kind[p] == DRV_AND) fl[p] = 1 + std::max(fl[g.fa[p] >> 1], fl[g.fb[p] >> 1]);
+    std::vector<uint8_t> stg(N + 1, 0);
+    for (uint32_t p = 0; p <= N; ++p) stg[p] = is_staged(p) ? 1 : 0;
+    // per block: edges i -> staged j with i later than j in the post-order
+    std::vector<int32_t> pos(N + 1, -1);
+    std::vector<uint32_t> touched, ss{0}, se;
+    for (size_t b0 = 0; b0 < E; b0 += 4096) {
+      const size_t b1 = std::min(E, b0 + 4096);
+      touched.clear();
+      repcut_topo(g, stg, ep.data() + es[b0], es[b1] - es[b0], pos, touched);
+      for (uint32_t j : touched) {
+        if (!stg[j] || g.kind[j] != DRV_AND) continue;
+        for (uint32_t f : {g.fa[j] >> 1, g.fb[j] >> 1}) {
+          if (!f || pos[f] < 0 || pos[f] <= pos[j]) continue;
+          for (uint32_t k = fs[f]; k < fs[f + 1]; ++k)
+            if (fo[k] == j) se.push_back(k);
+        }
+      }
+      for (uint32_t u : touched) pos[u] = -1;
+      ss.push_back((uint32_t)se.size());
+    }
+    std::vector<uint8_t> ws(N + 1, 0);
+    touched.clear();
+    repcut_topo(g, stg, ep.data(), ep.size(), pos, touched);
+    for (uint32_t j : touched) {
+      if (!stg[j] || g.kind[j] != DRV_AND) continue;
+      const uint32_t a = g.fa[j] >> 1, b = g.fb[j] >> 1;
+      if (a && pos[a] > pos[j]) ws[j] |= 1;
+      if (b && pos[b] > pos[j]) ws[j] |= 2;
+    }
+    if (sizes) {
+      sizes[0] = E;
+      sizes[1] = fo.size();
+      sizes[2] = ep.size();
+      sizes[3] = se.size();
+    }
+    if (supp_start) std::copy(ss.begin(), ss.end(), supp_start);
+    if (supp_edges) std::copy(se.begin(), se.end(), supp_edges);
+    if (wsupp) std::copy(ws.begin(), ws.end(), wsupp);
+    if (fanout_start) std::copy(fs.begin(), fs.end(), fanout_start);
+    if (fanouts) std::copy(fo.begin(), fo.end(), fanouts);
+    if (ep_start) std::copy(es.begin(), es.end(), ep_start);
+    if (ep_pins) std::copy(ep.begin(), ep.end(), ep_pins);
+    if (staged)
+      for (uint32_t p = 0; p <= N; ++p) staged[p] = is_staged(p) ? 1 : 0;
+    if (rlevel) std::copy(rl.begin(), rl.end(), rlevel);
+    if (flevel) std::copy(fl.begin(), fl.end(), flevel);
+    return (int64_t)st.size();
+  } catch (...) {
+    return -1;
+  }
 }
 
 int jqf_script_features(void *dp, void *sp, float *out) {

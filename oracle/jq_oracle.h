@@ -128,6 +128,16 @@ int jqo_aig_simulate(uint32_t num_pins, const uint8_t *kind, const uint32_t *fa,
                      size_t n_po, const uint32_t *po_iv, uint8_t *po_vals,
                      uint32_t *sram_words, uint8_t *sram_rd);
 
+/* RepCut endpoint-set clusters and endpoint weights of one staged slice
+ * (src/repcut.rs:58-176), from the arrays of jqf_repcut_slice.  Returns the
+ * number of clusters (class_of_pin, cluster_first, cluster_count filled in
+ * first-occurrence order), or -1. */
+int jqo_repcut(uint32_t num_pins, const uint8_t *kind, const uint32_t *fa, const uint32_t *fb,
+               const uint32_t *fanout_start, const uint32_t *fanouts, const uint8_t *staged,
+               uint32_t num_endpoints, const uint32_t *ep_start, const uint32_t *ep_pins,
+               int32_t *class_of_pin, uint32_t *cluster_first, uint32_t *cluster_count,
+               uint64_t *endpoint_weight);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,3 +103,28 @@ def aig_simulate(design, input_layout, in_vals, dff_init, num_cycles):
                        _p(q), int(design.num_srams), _p(sr), n_in, _p(lay), num_cycles, _p(inv),
                        _p(dff), n_po, _p(po), _p(pov), _p(sram_words), _p(sram_rd))
     return dff, pov
+
+
+def repcut(inp):
+    """jqo_repcut on the arrays of jacquard_b200.repcut.slice_inputs:
+    (class of each pin or -1, cluster first pins, cluster sizes, endpoint
+    weights)."""
+    L = lib()
+    if not getattr(L, "_jq_repcut_typed", False):
+        vp = ctypes.c_void_p
+        L.jqo_repcut.restype = ctypes.c_int
+        L.jqo_repcut.argtypes = [ctypes.c_uint32, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, vp, vp,
+                                 vp, vp, vp, vp]
+        L._jq_repcut_typed = True
+    N, E = inp["num_pins"], inp["num_endpoints"]
+    cls = np.zeros(N + 1, np.int32)
+    first = np.zeros(N + 1, np.uint32)
+    count = np.zeros(N + 1, np.uint32)
+    ew = np.zeros(max(1, E), np.uint64)
+    arrs = [np.ascontiguousarray(inp[k]) for k in ("kind", "fa", "fb", "fanout_start", "fanouts", "staged")]
+    n = L.jqo_repcut(N, *(a.ctypes.data for a in arrs), E, inp["ep_start"].ctypes.data,
+                     inp["ep_pins"].ctypes.data, cls.ctypes.data, first.ctypes.data, count.ctypes.data,
+                     ew.ctypes.data)
+    if n < 0:
+        raise MemoryError("repcut oracle")
+    return cls.astype(np.int64), first[:n].astype(np.int64), count[:n].astype(np.int64), ew[:E]
