@@ -158,6 +158,11 @@ typedef struct {
   size_t grid;                 /* CTAs; 0 = all that fit */
   uint64_t barrier_timeout_cycles;
   void *stream;
+  uint32_t lanes_per_item;     /* lane words one work item runs: 0 = automatic
+                                  (2 when lanes is even and the shared memory
+                                  of a lane pair fits the writeouts, else 1),
+                                  1, or 2 (JQ_ERR_INVALID_ARG when it does not
+                                  fit or lanes is odd) */
 } jq_batch_args;
 
 /* Prepares a script (FlattenedScriptV1, device arrays) for the batched

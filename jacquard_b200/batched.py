@@ -27,7 +27,8 @@ class BatchArgs(ctypes.Structure):
                 ("wo_slots", ctypes.c_uint32), ("block_list", vp), ("block_list_start", vp),
                 ("part_cycles", vp), ("part_base", vp), ("gr_sources", vp),
                 ("grid", ctypes.c_size_t),
-                ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp)]
+                ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp),
+                ("lanes_per_item", ctypes.c_uint32)]
 
 
 def lib():
@@ -123,7 +124,7 @@ class BatchedSim:
     """Script + buffers on the device for `lanes` lane words (32*lanes streams)."""
 
     def __init__(self, script, lanes, device="cuda", record=False, po_signals=None, grid=0,
-                 wo_slots=None):
+                 wo_slots=None, lanes_per_item=0):
         self.script = script
         self.lanes = lanes
         self.device = torch.device(device)
@@ -176,6 +177,9 @@ class BatchedSim:
         self.n_po = 0 if po_signals is None else len(po_signals)
         self.record = record
         self.grid = grid
+        # lane words per work item: 0 lets the library pick (lane pairs when
+        # lanes is even and they fit), 1 or 2 forces one
+        self.lanes_per_item = lanes_per_item
 
     def load_state(self, snap0):
         """snap0: (lanes, sig) u32 batched snapshot 0 (values + X template)."""
@@ -218,7 +222,8 @@ class BatchedSim:
                       part_cycles.data_ptr() if part_cycles is not None else None,
                       self.part_base_dev.data_ptr(), self.gr_sources.data_ptr(),
                       self.grid, 0,
-                      stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+                      stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream,
+                      self.lanes_per_item)
         rc = L.jq_simulate_batched(ctypes.byref(a))
         if rc:
             raise RuntimeError("jq_simulate_batched: " + sim.lib().jq_strerror(rc).decode())

@@ -468,20 +468,295 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
 }
 #undef JQ_FAIL_IF
 
-template <bool DS>
+// X-propagating AND of two lane words at once: (v0, x0, v1, x1) operands.
+__device__ __forceinline__ uint4 xand2(uint4 a, uint4 b, uint32_t xa, uint32_t xb, uint32_t ob) {
+  uint4 r;
+  xand(a.x, a.y, b.x, b.y, xa, xb, ob, r.x, r.y);
+  xand(a.z, a.w, b.z, b.w, xa, xb, ob, r.z, r.w);
+  return r;
+}
+__device__ __forceinline__ uint4 shfl4(uint4 v, uint32_t src) {
+  return make_uint4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                    __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+__device__ __forceinline__ uint4 shfl4_xor(uint4 v, uint32_t m) {
+  return make_uint4(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m),
+                    __shfl_xor_sync(0xffffffffu, v.z, m), __shfl_xor_sync(0xffffffffu, v.w, m));
+}
+
+// A lane-pair work item: the block's partition list for lane words 2lp and
+// 2lp+1 together.  Same steps as run_item; every tree position, writeout and
+// staged word holds (v0, x0, v1, x1), so the script chunks, the flag masks,
+// the barriers and the load latencies of a stage are shared by both lane
+// words.  The tree state is single-buffered (128 KB), so a barrier separates
+// the gathers of a stage from its first writes.
+__device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO, uint32_t *chunks,
+                          uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
+                          const uint32_t *in, uint32_t *out, uint32_t lp, uint32_t pid0,
+                          bool &failed, uint32_t &next_ticket, bool &have_next) {
+  const int t = threadIdx.x;
+  const size_t base0 = (size_t)(2 * lp) * P.sig_per_snap, base1 = base0 + P.sig_per_snap;
+  size_t off = 0;
+  uint32_t pid = pid0;
+  for (;;) {
+    __syncthreads();
+    const long long t_start = clock64();
+    if (t < 256) sh.meta[t] = __ldg(script + off + t);
+    uint32_t e[16];
+    {
+      const uint32_t *src = P.gr_sources + (size_t)pid * 8192;
+#pragma unroll
+      for (int k = 0; k < 16; ++k) e[k] = __ldg(src + t + BT * k);
+    }
+    __syncthreads();
+    const uint32_t ns = sh.meta[0];
+    if (!ns) break;
+    const uint32_t is_last = sh.meta[1], num_ios = sh.meta[2], io_off = sh.meta[3];
+    const uint32_t num_srams = sh.meta[4], sram_off = sh.meta[5], R = sh.meta[6];
+    const uint32_t num_dup = sh.meta[7];
+    const bool is_x = sh.meta[8] != 0;
+    const uint32_t xsig = sh.meta[9] * 32u;
+    const uint32_t *ch0 = script + off + 256 + 512 * (size_t)R;
+    const bool has_sram = (num_srams | num_dup) != 0;
+    const uint32_t nchunks = ns + (has_sram ? 2 : 1);
+    if (t == 0) {
+      mbar_expect_tx(&sh.bar[0], CHUNK_BYTES);
+      tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
+    }
+    // ---- global read, both lane words, in two halves of 8 positions
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint4 v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t ek = e[8 * h + k];
+        v[k] = make_uint4(0, 0, 0, 0);
+        if (ek != 0xffffffffu) {
+          const uint32_t *bp = (ek >> 31) ? out : in;
+          const size_t sg = ek & 0x7fffffffu;
+          v[k].x = ldcg(bp + base0 + sg);
+          v[k].z = ldcg(bp + base1 + sg);
+          if (is_x) {
+            v[k].y = ldcg(bp + xsig + base0 + sg);
+            v[k].w = ldcg(bp + xsig + base1 + sg);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) S[sw(t + BT * (8 * h + k))] = v[k];
+    }
+    const uint32_t lane_i = t & 31, warp_i = t >> 5;
+    const uint32_t u = residue(t);
+    const uint32_t us = sw(u);
+    for (uint32_t ci = 0; ci < nchunks; ++ci) {
+      const uint32_t b = ci & 1;
+      uint32_t *C = chunks + b * STAGE_WORDS;
+      if (ci == 0) __syncthreads();  // global read complete
+      if (t == 0 && ci + 1 < nchunks) {
+        mbar_expect_tx(&sh.bar[b ^ 1], CHUNK_BYTES);
+        const uint32_t nxt = (!has_sram && ci + 1 == ns) ? ns + 1 : ci + 1;
+        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, CHUNK_BYTES,
+                    &sh.bar[b ^ 1]);
+      }
+      uint32_t &uses = b ? uses1 : uses0;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.timeout));
+      ++uses;
+#define JQ_FAIL_IF(cond)                                               \
+  if (__syncthreads_or(cond)) {                                        \
+    failed = true;                                                     \
+    if (t == 0) mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.timeout); \
+    return;                                                            \
+  }
+      if (ci < ns) {
+        // ---------------- boomerang stage ci
+        uint4 v1[8];
+        uint32_t A = 0, B = 0;
+        if (ok) {
+          const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
+          const uint4 pa = P4[t], pb = P4[BT + t];
+          const uint2 fl = reinterpret_cast<const uint2 *>(C + 4096)[t];
+          A = fl.x;
+          B = fl.y;
+          const uint32_t ia[8] = {pa.x & 0xffffu, pa.x >> 16, pa.y & 0xffffu, pa.y >> 16,
+                                  pa.z & 0xffffu, pa.z >> 16, pa.w & 0xffffu, pa.w >> 16};
+          const uint32_t ib[8] = {pb.x & 0xffffu, pb.x >> 16, pb.y & 0xffffu, pb.y >> 16,
+                                  pb.z & 0xffffu, pb.z >> 16, pb.w & 0xffffu, pb.w >> 16};
+#define JQ_L1(k) v1[k] = xand2(S[ia[k]], S[ib[k]], mk<k>(A), mk<16 + k>(A), mk<k>(B));
+          JQ_L1(0) JQ_L1(1) JQ_L1(2) JQ_L1(3) JQ_L1(4) JQ_L1(5) JQ_L1(6) JQ_L1(7)
+#undef JQ_L1
+        }
+        // single buffer: every gather done before the first overwrite
+        JQ_FAIL_IF(!ok)
+        {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) S[4096 + 512 * k + us] = v1[k];
+          uint4 v2[4];
+#define JQ_L2(k)                                                                   \
+  v2[k] = xand2(v1[k], v1[k + 4], mk<8 + k>(A), mk<24 + k>(A), mk<8 + k>(B));      \
+  S[2048 + 512 * k + us] = v2[k];
+          JQ_L2(0) JQ_L2(1) JQ_L2(2) JQ_L2(3)
+#undef JQ_L2
+          const uint4 v30 = xand2(v2[0], v2[2], mk<12>(A), mk<28>(A), mk<12>(B));
+          S[1024 + us] = v30;
+          const uint4 v31 = xand2(v2[1], v2[3], mk<13>(A), mk<29>(A), mk<13>(B));
+          S[1536 + us] = v31;
+          const uint4 v4 = xand2(v30, v31, mk<14>(A), mk<30>(A), mk<14>(B));
+          S[512 + us] = v4;
+          const uint32_t XA = mk<15>(A), XB = mk<31>(A), OB = mk<15>(B);
+          uint4 c = xand2(shfl4_xor(v4, 16), v4, XA, XB, OB);
+          if (lane_i >= 16) S[us] = c;
+#pragma unroll
+          for (int k = 3; k >= 0; --k) {
+            const uint32_t d = 1u << k;
+            const uint4 a = shfl4(c, (lane_i + d) & 31);
+            const uint4 bb = shfl4(c, (lane_i + 2 * d) & 31);
+            if (lane_i >= d && lane_i < 2 * d) {
+              c = xand2(a, bb, XA, XB, OB);
+              S[us] = c;
+            }
+          }
+        }
+        __syncthreads();
+        // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
+        if (t < 32) {
+          uint4 h = t < 16 ? S[sw(16 + t)] : make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+          for (int m = 0; m < 4; ++m) {
+            const uint32_t len = 8u >> m;
+            const uint4 bb = shfl4(h, (t + len) & 31);
+            if ((uint32_t)t < len) {
+              h = xand2(h, bb, 0u - ((B >> (16 + m)) & 1u), 0u - ((B >> (20 + m)) & 1u),
+                        0u - ((B >> (24 + m)) & 1u));
+              S[len + t] = h;
+            }
+          }
+          if (t == 0) S[0] = make_uint4(0, 0, 0, 0);
+        }
+        __syncthreads();
+        for (uint32_t slot = warp_i; slot < num_ios; slot += BT / 32) {
+          const uint32_t hw = sh.meta[128 + slot / 2];
+          const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+          if ((hook >> 8) == ci) WO[slot * 32 + lane_i] = S[sw((hook & 255u) * 32 + lane_i)];
+        }
+      } else if (has_sram && ci == ns) {
+        // ---------------- SRAM & duplicate permutation + SRAM ports
+        JQ_FAIL_IF(!ok)
+        uint4 *St = S;
+        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
+        const uint32_t nq = (num_srams * 4 + num_dup) * 32;
+        for (uint32_t q = t; q < nq; q += BT) {
+          const uint4 w = WO[perm_lin(C, q)];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q);
+          St[q] = make_uint4((w.x & ~set0) ^ inv, is_x ? (w.y & ~set0) : 0u, (w.z & ~set0) ^ inv,
+                             is_x ? (w.w & ~set0) : 0u);
+        }
+        __syncthreads();
+        // one warp per (SRAM, lane word of the pair), lane = stream
+        const int warp = t >> 5, ln = t & 31;
+        for (uint32_t ih = warp; ih < num_srams * 2; ih += BT / 32) {
+          const uint32_t i = ih >> 1, hsel = ih & 1;
+          const uint32_t *Aw = reinterpret_cast<const uint32_t *>(St + (4 * i) * 32) + 2 * hsel;
+          uint32_t ra = 0, wa = 0, en = 0, data = 0, datax = 0;
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            ra |= ((Aw[4 * k] >> ln) & 1u) << k;
+            wa |= ((Aw[4 * (16 + k)] >> ln) & 1u) << k;
+          }
+#pragma unroll 8
+          for (int k = 0; k < 32; ++k) {
+            en |= ((Aw[4 * (32 + k)] >> ln) & 1u) << k;
+            const uint2 dk = *reinterpret_cast<const uint2 *>(Aw + 4 * (64 + k));
+            data |= ((dk.x >> ln) & 1u) << k;
+            datax |= ((dk.y >> ln) & 1u) << k;
+          }
+          const size_t stream = (size_t)(2 * lp + hsel) * 32 + ln;
+          uint32_t *ram = P.sram + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS;
+          const uint32_t r = ldcg(ram + ra), w0 = ldcg(ram + wa);
+          uint32_t rx = 0;
+          const bool hx = is_x && P.sram_x != nullptr;
+          uint32_t *ramx = hx ? P.sram_x + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS
+                              : nullptr;
+          uint32_t w0x = 0;
+          if (hx) {
+            rx = ldcg(ramx + ra);
+            w0x = ldcg(ramx + wa);
+          }
+          ram[wa] = (w0 & ~en) | (data & en);
+          if (hx) ramx[wa] = (w0x & ~en) | (datax & en);
+          const uint32_t slotw = (num_ios - num_srams + i) * 32;
+          uint32_t *WOw = reinterpret_cast<uint32_t *>(WO);
+#pragma unroll 4
+          for (int k = 0; k < 32; ++k) {
+            const uint32_t word = __ballot_sync(0xffffffffu, (r >> k) & 1u);
+            const uint32_t wordx = __ballot_sync(0xffffffffu, (rx >> k) & 1u);
+            if (ln == k) {
+              WOw[4 * (slotw + k) + 2 * hsel] = word;
+              WOw[4 * (slotw + k) + 2 * hsel + 1] = is_x ? wordx : 0u;
+            }
+          }
+        }
+        for (uint32_t q = t; q < num_dup * 32; q += BT)
+          WO[(num_ios - num_srams - num_dup) * 32 + q] = St[num_srams * 4 * 32 + q];
+        __syncthreads();
+      } else {
+        // ---------------- clock-enable permutation and commit, both lane words
+        JQ_FAIL_IF(!ok)
+        if (t == 0 && is_last) {
+          next_ticket = atomicAdd(&g_ticket[P.slot], 1u);
+          have_next = true;
+        }
+        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
+        const uint32_t nq = num_ios * 32;
+        for (uint32_t q = t; q < nq; q += BT) {
+          const uint4 src = WO[perm_lin(C, q)];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q), dinv = bitmask(fl.z, q);
+          const uint4 me = WO[q];
+          const size_t sg = (size_t)io_off * 32 + q;
+          const uint32_t old0 = ldcg(in + base0 + sg), old1 = ldcg(in + base1 + sg);
+          const uint32_t oldx0 = is_x ? ldcg(in + xsig + base0 + sg) : 0u;
+          const uint32_t oldx1 = is_x ? ldcg(in + xsig + base1 + sg) : 0u;
+          const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
+          out[base0 + sg] = (old0 & ~cp0) | ((me.x ^ dinv) & cp0);
+          out[base1 + sg] = (old1 & ~cp1) | ((me.z ^ dinv) & cp1);
+          if (is_x) {
+            const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
+            out[xsig + base0 + sg] = (oldx0 & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0;
+            out[xsig + base1 + sg] = (oldx1 & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1;
+          }
+        }
+      }
+    }
+    off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    if (P.part_cycles) {
+      __syncthreads();
+      if (t == 0) atomicAdd(&P.part_cycles[pid], (unsigned long long)(clock64() - t_start));
+    }
+    ++pid;
+    if (is_last) break;
+  }
+}
+#undef JQ_FAIL_IF
+
+// NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
+template <bool DS, int NL>
 __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
+  static_assert(NL == 1 || (NL == 2 && !DS), "lane pairs use a single tree buffer");
   extern __shared__ __align__(128) uint8_t dyn[];
   __shared__ Shared sh;
+  constexpr size_t WB = NL == 2 ? 16 : 8;  // bytes per tree / writeout word
   uint32_t *chunks = reinterpret_cast<uint32_t *>(dyn);               // 2 x 20 KB
-  uint2 *S = reinterpret_cast<uint2 *>(chunks + 2 * STAGE_WORDS);      // (1 or 2) x 8192 (v, x)
-  uint2 *WO = S + (DS ? 2 * 8192 : 8192);                             // wo_slots*32
+  uint8_t *S = dyn + 2 * CHUNK_BYTES;                                  // (1 or 2) x 8192 words
+  uint8_t *WO = S + (DS ? 2 : 1) * 8192 * WB;                          // wo_slots*32 words
   const int t = threadIdx.x;
   if (t == 0) {
     mbar_init(&sh.bar[0], 1);
     mbar_init(&sh.bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (uint32_t q = t; q < P.wo_slots * 32; q += BT) WO[q] = make_uint2(0, 0);
+  for (uint32_t q = t; q < P.wo_slots * 32 * (uint32_t)(WB / 4); q += BT)
+    reinterpret_cast<uint32_t *>(WO)[q] = 0;
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
@@ -513,7 +788,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
     for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
       const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
                                          : P.num_blocks;
-      const uint32_t items = nblk * P.lanes;
+      const uint32_t per = P.lanes / NL;  // items per block
+      const uint32_t items = nblk * per;
       uint32_t next_ticket = 0;
       bool have_next = false;
       for (;;) {
@@ -523,12 +799,16 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         have_next = false;
         const uint32_t tk = sh.ticket;
         if (tk >= items) break;
-        const uint32_t bi = tk / P.lanes, lane = tk % P.lanes;
+        const uint32_t bi = tk / per, lane = tk % per;
         const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
         const uint32_t *script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
         const uint32_t pid0 = P.part_base[(size_t)ms * P.num_blocks + blk];
-        run_item<DS>(P, sh, S, WO, chunks, uses0, uses1, script, in, out, lane, pid0, failed,
-                     next_ticket, have_next);
+        if constexpr (NL == 2)
+          run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
+                    uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next);
+        else
+          run_item<DS>(P, sh, reinterpret_cast<uint2 *>(S), reinterpret_cast<uint2 *>(WO), chunks,
+                       uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next);
         if (failed) {
           if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
           return;
@@ -709,29 +989,49 @@ __global__ void jq_batched_reset_kernel(int slot) {
 
 extern "C" {
 
-static size_t smem_layout_bytes(uint32_t wo_slots, bool ds) {
-  return 2 * (size_t)CHUNK_BYTES + (ds ? 2 : 1) * 8192 * 8 + (size_t)wo_slots * 32 * 8;
+// Kernel variant: lane words per work item and tree-state buffering.
+struct Variant {
+  int nl;   // 1 or 2 lane words per item
+  bool ds;  // double-buffered tree state (nl == 1 only)
+};
+
+static const void *variant_fn(Variant v) {
+  if (v.nl == 2) return (const void *)jq_batched_kernel<false, 2>;
+  return v.ds ? (const void *)jq_batched_kernel<true, 1> : (const void *)jq_batched_kernel<false, 1>;
 }
 
-// Double-buffered tree state when it fits next to the writeouts.
-static bool use_double_buffer(uint32_t wo_slots) {
+static size_t smem_layout_bytes(uint32_t wo_slots, Variant v) {
+  const size_t wb = v.nl == 2 ? 16 : 8;
+  return 2 * (size_t)CHUNK_BYTES + (v.ds ? 2 : 1) * 8192 * wb + (size_t)wo_slots * 32 * wb;
+}
+
+static bool variant_fits(uint32_t wo_slots, Variant v) {
   int dev = 0, optin = 0;
   cudaFuncAttributes fa;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-      cudaFuncGetAttributes(&fa, jq_batched_kernel<true>) != cudaSuccess)
+      cudaFuncGetAttributes(&fa, variant_fn(v)) != cudaSuccess)
     return false;
-  return smem_layout_bytes(wo_slots, true) + fa.sharedSizeBytes <= (size_t)optin;
+  return smem_layout_bytes(wo_slots, v) + fa.sharedSizeBytes <= (size_t)optin;
+}
+
+// want_nl 0 = automatic: lane pairs when the lane count is even and their
+// shared memory fits, else single lanes, double-buffered when that fits.
+// nl = 0 in the result: the requested variant is not possible.
+static Variant pick_variant(uint32_t wo_slots, uint32_t lanes, uint32_t want_nl) {
+  if (want_nl != 1 && lanes % 2 == 0 && variant_fits(wo_slots, Variant{2, false}))
+    return Variant{2, false};
+  if (want_nl == 2) return Variant{0, false};
+  return Variant{1, variant_fits(wo_slots, Variant{1, true})};
 }
 
 int jq_batched_smem_bytes(uint32_t wo_slots) {
-  return (int)smem_layout_bytes(wo_slots, use_double_buffer(wo_slots));
+  return (int)smem_layout_bytes(wo_slots, pick_variant(wo_slots, 1, 1));
 }
 
-int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
-  const bool ds = use_double_buffer(wo_slots);
-  const void *fn = ds ? (const void *)jq_batched_kernel<true> : (const void *)jq_batched_kernel<false>;
-  int smem = (int)smem_layout_bytes(wo_slots, ds);
+static int variant_max_blocks(int device, uint32_t wo_slots, Variant v, size_t *max_blocks) {
+  const void *fn = variant_fn(v);
+  const int smem = (int)smem_layout_bytes(wo_slots, v);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
     return JQ_ERR_LAUNCH;
   int sms = 0, per = 0;
@@ -740,6 +1040,11 @@ int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
     return JQ_ERR_LAUNCH;
   *max_blocks = (size_t)sms * per;
   return JQ_OK;
+}
+
+int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
+  // every variant runs one CTA per SM
+  return variant_max_blocks(device, wo_slots, pick_variant(wo_slots, 1, 1), max_blocks);
 }
 
 size_t jq_batched_gr_words(size_t num_partitions) { return (num_partitions + 1) * 8192; }
@@ -798,8 +1103,11 @@ int jq_simulate_batched(const jq_batch_args *a) {
   int dev = 0;
   cudaGetDevice(&dev);
   const uint32_t wo_slots = a->wo_slots ? a->wo_slots : 256;
+  if (a->lanes_per_item > 2) return JQ_ERR_INVALID_ARG;
+  const Variant v = pick_variant(wo_slots, a->lanes, a->lanes_per_item);
+  if (v.nl == 0) return JQ_ERR_INVALID_ARG;
   size_t maxg = 0;
-  if (jq_batched_max_blocks(dev, wo_slots, &maxg) != JQ_OK || maxg == 0) return JQ_ERR_LAUNCH;
+  if (variant_max_blocks(dev, wo_slots, v, &maxg) != JQ_OK || maxg == 0) return JQ_ERR_LAUNCH;
   size_t grid = a->grid ? a->grid : maxg;
   if (grid > maxg) return JQ_ERR_TOO_MANY_BLOCKS;
   BatchParams P;
@@ -834,12 +1142,9 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.slot = 1;
   jq_batched_reset_kernel<<<1, 1, 0, st>>>(P.slot);
   if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
-  const bool ds = use_double_buffer(P.wo_slots);
-  int smem = (int)smem_layout_bytes(P.wo_slots, ds);
+  const int smem = (int)smem_layout_bytes(P.wo_slots, v);
   void *args[] = {&P};
-  cudaError_t e = cudaLaunchCooperativeKernel(
-      ds ? (void *)jq_batched_kernel<true> : (void *)jq_batched_kernel<false>, (unsigned)grid, BT,
-      args, smem, st);
+  cudaError_t e = cudaLaunchCooperativeKernel(variant_fn(v), (unsigned)grid, BT, args, smem, st);
   return e == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
 }
 

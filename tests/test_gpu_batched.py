@@ -17,13 +17,17 @@ def per_stream_states(kind, s, cycles, streams, x_init):
     return np.stack(out)  # (S, cycles+1, eff)
 
 
-@pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots", [
-    ("tiny", 8, (5,), False, 1, None),
-    ("sram", 16, (8,), True, 2, None),
-    ("sram", 16, (8,), True, 1, 256),  # single-buffered tree state
-    ("soc_mini", 148, (20, 40, 60), True, 1, None),
+@pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots,per_item", [
+    ("tiny", 8, (5,), False, 1, None, 0),
+    ("sram", 16, (8,), True, 2, None, 0),     # lane pairs
+    ("sram", 16, (8,), True, 2, None, 1),     # single lanes, double-buffered tree
+    ("sram", 16, (8,), True, 1, 256, 0),      # single-buffered tree state
+    ("sram", 16, (8,), True, 2, 256, 0),      # lane pairs do not fit: single lanes
+    ("tiny", 8, (5,), False, 4, None, 2),
+    ("soc_mini", 148, (20, 40, 60), True, 1, None, 0),
+    ("soc_mini", 148, (20, 40, 60), True, 2, None, 0),
 ])
-def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slots):
+def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slots, per_item):
     s = cases.script(kind, nb, split, xprop=xprop)
     cycles = 10
     S = 32 * lanes
@@ -40,7 +44,7 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slo
         want[k] = st.reshape(cycles + 1, eff)
         wsram.append(sram)
     # batched
-    B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots)
+    B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots, lanes_per_item=per_item)
     bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
     B.load_state(bt[0])
     B.reset_sram()
@@ -56,6 +60,14 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slo
     gs = B.sram.cpu().numpy().view(np.uint32).reshape(S, -1)
     for k in range(S):
         assert np.array_equal(gs[k][: wsram[k].size], wsram[k])
+
+
+def test_lane_pairs_rejected_for_odd_lanes():
+    s = cases.script("tiny", 8, (5,), xprop=False)
+    B = batched.BatchedSim(s, 1, lanes_per_item=2)
+    stim = None
+    with pytest.raises(RuntimeError):
+        B.run(stim, 1)
 
 
 def test_layout_roundtrip():
