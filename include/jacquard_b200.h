@@ -148,7 +148,8 @@ typedef struct {
                                   for all blocks */
   const uint32_t *block_list_start; /* device: num_major_stages+1 offsets */
   unsigned long long *part_cycles; /* optional device output: SM clocks spent
-                                      per partition, summed over lanes and
+                                      per partition, summed over work items
+                                      (a lane-pair item counts once) and
                                       cycles (partition order of the script:
                                       major stage, block, position in block) */
   const uint32_t *part_base;   /* device: index of the first partition of each

@@ -33,6 +33,9 @@ constexpr int BT = 512;  // threads per CTA
 constexpr uint32_t CHUNK_BYTES = STAGE_WORDS * 4;
 
 static __device__ unsigned int g_ticket[BAR_SLOTS];
+// Global-read source table sentinels (jq_batched_prepare).
+constexpr uint32_t GR_EMPTY = 0xffffffffu;  // needed, no source: stored as 0
+constexpr uint32_t GR_SKIP = 0xfffffffeu;   // not needed by any gather
 
 struct BatchParams {
   unsigned num_blocks, num_major_stages, lanes;
@@ -198,16 +201,16 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
 
     // ---- global read into tree buffer 0.  The source signal of every
     // position (the kernel's bit-append order, resolved once per script by
-    // jq_batched_prepare; bit 31 = current-cycle staged IO, all ones = none)
-    // was loaded at the top of the partition; 32 independent state loads per
-    // thread follow.
+    // jq_batched_prepare; bit 31 = current-cycle staged IO, GR_EMPTY = none,
+    // GR_SKIP = read by no needed gather) was loaded at the top of the
+    // partition; up to 32 independent state loads per thread follow.
     {
       uint32_t v[16], vx[16];
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
         v[k] = 0;
         vx[k] = 0;
-        if (e[k] != 0xffffffffu) {
+        if (e[k] < GR_SKIP) {
           const uint32_t *base = (e[k] >> 31) ? out : in;
           const size_t sg = lane_base + (e[k] & 0x7fffffffu);
           v[k] = ldcg(base + sg);
@@ -215,7 +218,8 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         }
       }
 #pragma unroll
-      for (int k = 0; k < 16; ++k) Sb0[sw(t + BT * k)] = make_uint2(v[k], vx[k]);
+      for (int k = 0; k < 16; ++k)
+        if (e[k] != GR_SKIP) Sb0[sw(t + BT * k)] = make_uint2(v[k], vx[k]);
     }
 
     // Thread -> tree residue map: thread (warp w, lane l) owns positions whose
@@ -256,97 +260,109 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         const uint2 *Sp = (ci & 1) ? Sb1 : Sb0;
         uint2 *Sn = (ci & 1) ? Sb0 : Sb1;
         uint2 ga[8], gb[8];
-        uint32_t A = 0, B = 0;
+        uint32_t A = 0, B = 0, sm = 0;
+        // no position below 512 live: levels 5..13 are skipped (uniform:
+        // every thread's entry 0 carries it)
+        bool shallow = false;
         if (ok) {
           const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
           const uint4 pa = P4[t], pb = P4[BT + t];
           const uint2 fl = reinterpret_cast<const uint2 *>(C + 4096)[t];
           A = fl.x;
           B = fl.y;
-          ga[0] = Sp[pa.x & 0xffffu]; ga[1] = Sp[pa.x >> 16];
-          ga[2] = Sp[pa.y & 0xffffu]; ga[3] = Sp[pa.y >> 16];
-          ga[4] = Sp[pa.z & 0xffffu]; ga[5] = Sp[pa.z >> 16];
-          ga[6] = Sp[pa.w & 0xffffu]; ga[7] = Sp[pa.w >> 16];
-          gb[0] = Sp[pb.x & 0xffffu]; gb[1] = Sp[pb.x >> 16];
-          gb[2] = Sp[pb.y & 0xffffu]; gb[3] = Sp[pb.y >> 16];
-          gb[4] = Sp[pb.z & 0xffffu]; gb[5] = Sp[pb.z >> 16];
-          gb[6] = Sp[pb.w & 0xffffu]; gb[7] = Sp[pb.w >> 16];
+          shallow = (pa.x >> 13) & 1u;
+          sm = t < 8 ? 0xffffu : (B >> 16);  // owned positions to store
+          // gathers the prepared liveness marks as not needed read nothing
+#define JQ_G(dst, w, h) \
+  dst = (((w) >> (16 * (h) + 15)) & 1u) ? Sp[((w) >> (16 * (h))) & 0x1fffu] : make_uint2(0, 0);
+          JQ_G(ga[0], pa.x, 0) JQ_G(ga[1], pa.x, 1) JQ_G(ga[2], pa.y, 0) JQ_G(ga[3], pa.y, 1)
+          JQ_G(ga[4], pa.z, 0) JQ_G(ga[5], pa.z, 1) JQ_G(ga[6], pa.w, 0) JQ_G(ga[7], pa.w, 1)
+          JQ_G(gb[0], pb.x, 0) JQ_G(gb[1], pb.x, 1) JQ_G(gb[2], pb.y, 0) JQ_G(gb[3], pb.y, 1)
+          JQ_G(gb[4], pb.z, 0) JQ_G(gb[5], pb.z, 1) JQ_G(gb[6], pb.w, 0) JQ_G(gb[7], pb.w, 1)
+#undef JQ_G
         }
         if (!ds) {
           // single buffer: all gathers done before the in-place overwrite
           JQ_FAIL_IF(!ok)
         }
         if (ok) {
-          // level 1 (positions 4096 + u + 512k)
+          // level 1 (positions 4096 + u + 512k); owned position i is stored
+          // only when read from outside its stage (bit i of sm)
           uint32_t v1[8], x1[8];
 #define JQ_L1(k)                                                                         \
   xand(ga[k].x, ga[k].y, gb[k].x, gb[k].y, mk<k>(A), mk<16 + k>(A), mk<k>(B), v1[k], x1[k]); \
-  Sn[4096 + 512 * k + us] = make_uint2(v1[k], x1[k]);
+  if (((sm >> (k)) & 1u)) Sn[4096 + 512 * k + us] = make_uint2(v1[k], x1[k]);
           JQ_L1(0) JQ_L1(1) JQ_L1(2) JQ_L1(3) JQ_L1(4) JQ_L1(5) JQ_L1(6) JQ_L1(7)
 #undef JQ_L1
           uint32_t v2[4], x2[4];
 #define JQ_L2(k)                                                                           \
   xand(v1[k], x1[k], v1[k + 4], x1[k + 4], mk<8 + k>(A), mk<24 + k>(A), mk<8 + k>(B), v2[k], \
        x2[k]);                                                                             \
-  Sn[2048 + 512 * k + us] = make_uint2(v2[k], x2[k]);
+  if (((sm >> (8 + k)) & 1u)) Sn[2048 + 512 * k + us] = make_uint2(v2[k], x2[k]);
           JQ_L2(0) JQ_L2(1) JQ_L2(2) JQ_L2(3)
 #undef JQ_L2
           uint32_t v3[2], x3[2];
           xand(v2[0], x2[0], v2[2], x2[2], mk<12>(A), mk<28>(A), mk<12>(B), v3[0], x3[0]);
-          Sn[1024 + us] = make_uint2(v3[0], x3[0]);
+          if (((sm >> 12) & 1u)) Sn[1024 + us] = make_uint2(v3[0], x3[0]);
           xand(v2[1], x2[1], v2[3], x2[3], mk<13>(A), mk<29>(A), mk<13>(B), v3[1], x3[1]);
-          Sn[1536 + us] = make_uint2(v3[1], x3[1]);
+          if (((sm >> 13) & 1u)) Sn[1536 + us] = make_uint2(v3[1], x3[1]);
           uint32_t v4, x4;
           xand(v3[0], x3[0], v3[1], x3[1], mk<14>(A), mk<30>(A), mk<14>(B), v4, x4);
-          Sn[512 + us] = make_uint2(v4, x4);
-          // levels 5..9: the thread's position u (u >= 16) at the level of
-          // its lane: level 5 (lanes 16..31) from level-4 residues u-256
-          // (lane ^ 16) and u; level 6+k' (lanes [2^k, 2^(k+1))) from lanes
-          // l + 2^k and l + 2^(k+1)
-          const uint32_t XA = mk<15>(A), XB = mk<31>(A), OB = mk<15>(B);
-          uint32_t cv, cx;
-          {
-            const uint32_t a = __shfl_xor_sync(0xffffffffu, v4, 16);
-            const uint32_t ax = __shfl_xor_sync(0xffffffffu, x4, 16);
-            xand(a, ax, v4, x4, XA, XB, OB, cv, cx);
-            if (lane_i >= 16) Sn[us] = make_uint2(cv, cx);
-          }
+          if (((sm >> 14) & 1u)) Sn[512 + us] = make_uint2(v4, x4);
+          if (shallow) {
+            if (t == 0) Sn[0] = make_uint2(0, 0);
+          } else {
+            // levels 5..9: the thread's position u (u >= 16) at the level of
+            // its lane: level 5 (lanes 16..31) from level-4 residues u-256
+            // (lane ^ 16) and u; level 6+k' (lanes [2^k, 2^(k+1))) from lanes
+            // l + 2^k and l + 2^(k+1)
+            const uint32_t XA = mk<15>(A), XB = mk<31>(A), OB = mk<15>(B);
+            uint32_t cv, cx;
+            {
+              const uint32_t a = __shfl_xor_sync(0xffffffffu, v4, 16);
+              const uint32_t ax = __shfl_xor_sync(0xffffffffu, x4, 16);
+              xand(a, ax, v4, x4, XA, XB, OB, cv, cx);
+              if (lane_i >= 16) Sn[us] = make_uint2(cv, cx);
+            }
 #pragma unroll
-          for (int k = 3; k >= 0; --k) {
-            const uint32_t d = 1u << k;
-            const uint32_t a = __shfl_sync(0xffffffffu, cv, (lane_i + d) & 31);
-            const uint32_t bb = __shfl_sync(0xffffffffu, cv, (lane_i + 2 * d) & 31);
-            const uint32_t ax = __shfl_sync(0xffffffffu, cx, (lane_i + d) & 31);
-            const uint32_t bx = __shfl_sync(0xffffffffu, cx, (lane_i + 2 * d) & 31);
-            if (lane_i >= d && lane_i < 2 * d) {
-              xand(a, ax, bb, bx, XA, XB, OB, cv, cx);
-              Sn[us] = make_uint2(cv, cx);
+            for (int k = 3; k >= 0; --k) {
+              const uint32_t d = 1u << k;
+              const uint32_t a = __shfl_sync(0xffffffffu, cv, (lane_i + d) & 31);
+              const uint32_t bb = __shfl_sync(0xffffffffu, cv, (lane_i + 2 * d) & 31);
+              const uint32_t ax = __shfl_sync(0xffffffffu, cx, (lane_i + d) & 31);
+              const uint32_t bx = __shfl_sync(0xffffffffu, cx, (lane_i + 2 * d) & 31);
+              if (lane_i >= d && lane_i < 2 * d) {
+                xand(a, ax, bb, bx, XA, XB, OB, cv, cx);
+                Sn[us] = make_uint2(cv, cx);
+              }
             }
           }
         }
         JQ_FAIL_IF(!ok)
-        // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
-        if (t < 32) {
-          uint2 h = t < 16 ? Sn[sw(16 + t)] : make_uint2(0, 0);
-          uint32_t hv = h.x, hx = h.y;
-          // rolled: this serial section runs in one warp, keep its code short
+        if (!shallow) {
+          // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
+          if (t < 32) {
+            uint2 h = t < 16 ? Sn[sw(16 + t)] : make_uint2(0, 0);
+            uint32_t hv = h.x, hx = h.y;
+            // rolled: this serial section runs in one warp, keep its code short
 #pragma unroll 1
-          for (int m = 0; m < 4; ++m) {
-            const uint32_t len = 8u >> m;
-            const uint32_t bb = __shfl_sync(0xffffffffu, hv, (t + len) & 31);
-            const uint32_t bx = __shfl_sync(0xffffffffu, hx, (t + len) & 31);
-            if ((uint32_t)t < len) {
-              uint32_t r, rx;
-              xand(hv, hx, bb, bx, 0u - ((B >> (16 + m)) & 1u), 0u - ((B >> (20 + m)) & 1u),
-                   0u - ((B >> (24 + m)) & 1u), r, rx);
-              Sn[len + t] = make_uint2(r, rx);
-              hv = r;
-              hx = rx;
+            for (int m = 0; m < 4; ++m) {
+              const uint32_t len = 8u >> m;
+              const uint32_t bb = __shfl_sync(0xffffffffu, hv, (t + len) & 31);
+              const uint32_t bx = __shfl_sync(0xffffffffu, hx, (t + len) & 31);
+              if ((uint32_t)t < len) {
+                uint32_t r, rx;
+                xand(hv, hx, bb, bx, 0u - ((B >> (16 + m)) & 1u), 0u - ((B >> (20 + m)) & 1u),
+                     0u - ((B >> (24 + m)) & 1u), r, rx);
+                Sn[len + t] = make_uint2(r, rx);
+                hv = r;
+                hx = rx;
+              }
             }
+            if (t == 0) Sn[0] = make_uint2(0, 0);
           }
-          if (t == 0) Sn[0] = make_uint2(0, 0);
+          __syncthreads();
         }
-        __syncthreads();
         // writeout hooks of this stage: warp w scans slots w, w+16, ...
         for (uint32_t slot = warp_i; slot < num_ios; slot += BT / 32) {
           const uint32_t hw = sh.meta[128 + slot / 2];
@@ -531,7 +547,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       for (int k = 0; k < 8; ++k) {
         const uint32_t ek = e[8 * h + k];
         v[k] = make_uint4(0, 0, 0, 0);
-        if (ek != 0xffffffffu) {
+        if (ek < GR_SKIP) {
           const uint32_t *bp = (ek >> 31) ? out : in;
           const size_t sg = ek & 0x7fffffffu;
           v[k].x = ldcg(bp + base0 + sg);
@@ -543,7 +559,8 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         }
       }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) S[sw(t + BT * (8 * h + k))] = v[k];
+      for (int k = 0; k < 8; ++k)
+        if (e[8 * h + k] != GR_SKIP) S[sw(t + BT * (8 * h + k))] = v[k];
     }
     const uint32_t lane_i = t & 31, warp_i = t >> 5;
     const uint32_t u = residue(t);
@@ -570,69 +587,81 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       if (ci < ns) {
         // ---------------- boomerang stage ci
         uint4 v1[8];
-        uint32_t A = 0, B = 0;
+        uint32_t A = 0, B = 0, sm = 0;
+        bool shallow = false;  // no position below 512 live
         if (ok) {
           const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
           const uint4 pa = P4[t], pb = P4[BT + t];
           const uint2 fl = reinterpret_cast<const uint2 *>(C + 4096)[t];
           A = fl.x;
           B = fl.y;
-          const uint32_t ia[8] = {pa.x & 0xffffu, pa.x >> 16, pa.y & 0xffffu, pa.y >> 16,
-                                  pa.z & 0xffffu, pa.z >> 16, pa.w & 0xffffu, pa.w >> 16};
-          const uint32_t ib[8] = {pb.x & 0xffffu, pb.x >> 16, pb.y & 0xffffu, pb.y >> 16,
-                                  pb.z & 0xffffu, pb.z >> 16, pb.w & 0xffffu, pb.w >> 16};
-#define JQ_L1(k) v1[k] = xand2(S[ia[k]], S[ib[k]], mk<k>(A), mk<16 + k>(A), mk<k>(B));
-          JQ_L1(0) JQ_L1(1) JQ_L1(2) JQ_L1(3) JQ_L1(4) JQ_L1(5) JQ_L1(6) JQ_L1(7)
+          shallow = (pa.x >> 13) & 1u;
+          sm = t < 8 ? 0xffffu : (B >> 16);
+#define JQ_G(w, h) \
+  ((((w) >> (16 * (h) + 15)) & 1u) ? S[((w) >> (16 * (h))) & 0x1fffu] : make_uint4(0, 0, 0, 0))
+#define JQ_L1(k, wa, wb, h) v1[k] = xand2(JQ_G(wa, h), JQ_G(wb, h), mk<k>(A), mk<16 + k>(A), mk<k>(B));
+          JQ_L1(0, pa.x, pb.x, 0) JQ_L1(1, pa.x, pb.x, 1) JQ_L1(2, pa.y, pb.y, 0)
+          JQ_L1(3, pa.y, pb.y, 1) JQ_L1(4, pa.z, pb.z, 0) JQ_L1(5, pa.z, pb.z, 1)
+          JQ_L1(6, pa.w, pb.w, 0) JQ_L1(7, pa.w, pb.w, 1)
 #undef JQ_L1
+#undef JQ_G
         }
         // single buffer: every gather done before the first overwrite
         JQ_FAIL_IF(!ok)
         {
-#pragma unroll
-          for (int k = 0; k < 8; ++k) S[4096 + 512 * k + us] = v1[k];
+#define JQ_ST1(k) \
+  if (((sm >> (k)) & 1u)) S[4096 + 512 * k + us] = v1[k];
+          JQ_ST1(0) JQ_ST1(1) JQ_ST1(2) JQ_ST1(3) JQ_ST1(4) JQ_ST1(5) JQ_ST1(6) JQ_ST1(7)
+#undef JQ_ST1
           uint4 v2[4];
 #define JQ_L2(k)                                                                   \
   v2[k] = xand2(v1[k], v1[k + 4], mk<8 + k>(A), mk<24 + k>(A), mk<8 + k>(B));      \
-  S[2048 + 512 * k + us] = v2[k];
+  if (((sm >> (8 + k)) & 1u)) S[2048 + 512 * k + us] = v2[k];
           JQ_L2(0) JQ_L2(1) JQ_L2(2) JQ_L2(3)
 #undef JQ_L2
           const uint4 v30 = xand2(v2[0], v2[2], mk<12>(A), mk<28>(A), mk<12>(B));
-          S[1024 + us] = v30;
+          if (((sm >> 12) & 1u)) S[1024 + us] = v30;
           const uint4 v31 = xand2(v2[1], v2[3], mk<13>(A), mk<29>(A), mk<13>(B));
-          S[1536 + us] = v31;
+          if (((sm >> 13) & 1u)) S[1536 + us] = v31;
           const uint4 v4 = xand2(v30, v31, mk<14>(A), mk<30>(A), mk<14>(B));
-          S[512 + us] = v4;
-          const uint32_t XA = mk<15>(A), XB = mk<31>(A), OB = mk<15>(B);
-          uint4 c = xand2(shfl4_xor(v4, 16), v4, XA, XB, OB);
-          if (lane_i >= 16) S[us] = c;
+          if (((sm >> 14) & 1u)) S[512 + us] = v4;
+          if (shallow) {
+            if (t == 0) S[0] = make_uint4(0, 0, 0, 0);
+          } else {
+            const uint32_t XA = mk<15>(A), XB = mk<31>(A), OB = mk<15>(B);
+            uint4 c = xand2(shfl4_xor(v4, 16), v4, XA, XB, OB);
+            if (lane_i >= 16) S[us] = c;
 #pragma unroll
-          for (int k = 3; k >= 0; --k) {
-            const uint32_t d = 1u << k;
-            const uint4 a = shfl4(c, (lane_i + d) & 31);
-            const uint4 bb = shfl4(c, (lane_i + 2 * d) & 31);
-            if (lane_i >= d && lane_i < 2 * d) {
-              c = xand2(a, bb, XA, XB, OB);
-              S[us] = c;
+            for (int k = 3; k >= 0; --k) {
+              const uint32_t d = 1u << k;
+              const uint4 a = shfl4(c, (lane_i + d) & 31);
+              const uint4 bb = shfl4(c, (lane_i + 2 * d) & 31);
+              if (lane_i >= d && lane_i < 2 * d) {
+                c = xand2(a, bb, XA, XB, OB);
+                S[us] = c;
+              }
             }
           }
         }
         __syncthreads();
-        // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
-        if (t < 32) {
-          uint4 h = t < 16 ? S[sw(16 + t)] : make_uint4(0, 0, 0, 0);
+        if (!shallow) {
+          // levels 10..13 (positions 15..1) in warp 0 from positions 16..31
+          if (t < 32) {
+            uint4 h = t < 16 ? S[sw(16 + t)] : make_uint4(0, 0, 0, 0);
 #pragma unroll 1
-          for (int m = 0; m < 4; ++m) {
-            const uint32_t len = 8u >> m;
-            const uint4 bb = shfl4(h, (t + len) & 31);
-            if ((uint32_t)t < len) {
-              h = xand2(h, bb, 0u - ((B >> (16 + m)) & 1u), 0u - ((B >> (20 + m)) & 1u),
-                        0u - ((B >> (24 + m)) & 1u));
-              S[len + t] = h;
+            for (int m = 0; m < 4; ++m) {
+              const uint32_t len = 8u >> m;
+              const uint4 bb = shfl4(h, (t + len) & 31);
+              if ((uint32_t)t < len) {
+                h = xand2(h, bb, 0u - ((B >> (16 + m)) & 1u), 0u - ((B >> (20 + m)) & 1u),
+                          0u - ((B >> (24 + m)) & 1u));
+                S[len + t] = h;
+              }
             }
+            if (t == 0) S[0] = make_uint4(0, 0, 0, 0);
           }
-          if (t == 0) S[0] = make_uint4(0, 0, 0, 0);
+          __syncthreads();
         }
-        __syncthreads();
         for (uint32_t slot = warp_i; slot < num_ios; slot += BT / 32) {
           const uint32_t hw = sh.meta[128 + slot / 2];
           const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
@@ -866,9 +895,32 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 // clock-enable chunks get their shuffle entries in q order.  Metadata, global
 // read sections and sizes are unchanged, so blocks_start stays valid.  One
 // CTA per (major stage, block) entry walks its partition list.
+//
+// Liveness.  A tree position is read from outside its stage when a writeout
+// hook of the stage covers it or a needed gather of the next stage names it;
+// it is live when it is read from outside or its parent is live (each
+// position has one parent: children [2L, 3L) are the a inputs and [3L, 4L)
+// the b inputs of [L, 2L)).  A level-1 input is needed when its position is
+// live, except a b input whose ob flag forces it to one.  Stages are walked
+// last to first, so each stage's needed gathers give the previous stage's
+// externally read positions (for stage 0: the global-read positions).  The
+// source entries are 13-bit tree addresses; their top bits carry
+//   bit 15  the gather is needed (otherwise the kernel reads nothing and
+//           uses 0, which only feeds dead positions or an ob-forced input);
+//   bit 13  of entry 0: no position below 512 is live (levels 5..13 skipped).
+// Bits 16+i of the second flag word of threads t >= 8 mark owned position i
+// as read from outside its stage; only those are stored (threads t < 8 hold
+// the warp-0 flags there and store all their positions).
+// Unneeded global-read positions get source 0xfffffffe (neither loaded nor
+// stored).  Dead positions are neither stored nor read, so the state they
+// leave in shared memory is never observed.
+
 __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     const size_t *blocks_start, const uint32_t *src, uint32_t *dst, unsigned entries,
     const uint32_t *part_base, uint32_t *gr_sources, size_t num_partitions) {
+  __shared__ uint32_t need_bits[256];  // previous tree's positions read by needed gathers
+  __shared__ uint32_t ext_bits[256];   // this stage's positions read from outside
+  __shared__ uint8_t live[8192];
   const unsigned e = blockIdx.x;
   if (e >= entries) return;
   const uint32_t t = threadIdx.x;
@@ -878,11 +930,92 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
   for (;;) {
     const uint32_t ns = src[off];
     if (!ns || pid >= num_partitions) break;
-    const uint32_t is_last = src[off + 1], R = src[off + 6];
+    const uint32_t is_last = src[off + 1], nio = src[off + 2], R = src[off + 6];
+    const uint32_t *ch = src + off + 256 + 512 * (size_t)R;
+    uint32_t *dch = dst + off + 256 + 512 * (size_t)R;
+    for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;  // nothing reads the last stage
+    __syncthreads();
+    for (int ci = (int)ns - 1; ci >= 0; --ci) {
+      const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
+      uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
+      for (uint32_t w = t; w < 256; w += BT) ext_bits[w] = need_bits[w];
+      __syncthreads();
+      for (uint32_t slot = t; slot < nio; slot += BT) {
+        const uint32_t hw = src[off + 128 + slot / 2];
+        const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+        if ((hook >> 8) == (uint32_t)ci) ext_bits[hook & 255u] = 0xffffffffu;
+      }
+      __syncthreads();
+      // top-down, one level per pass: position 1, then [2, 4), ..., [4096, 8192)
+      if (t == 0) live[0] = 0;
+      for (uint32_t M = 1; M <= 4096; M <<= 1) {
+        for (uint32_t c = M + t; c < 2 * M; c += BT) {
+          uint8_t l = (uint8_t)((ext_bits[c >> 5] >> (c & 31)) & 1u);
+          if (M > 1) {
+            const uint32_t h = M >> 1;
+            l |= live[c < M + h ? c - h : c - M];
+          }
+          live[c] = l;
+        }
+        __syncthreads();
+      }
+      const int deep = __syncthreads_or(t > 0 && live[t]);  // BT = 512
+      for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        // plane m>>2, word m&3: entries 8*(m>>2) + 2*(m&3) + {0, 1}; entry
+        // k < 8 is input a of position 4096+u+512k (source q = u+512k),
+        // entry 8+k its input b (q + 4096)
+        uint32_t w = 0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t en = 8 * (m >> 2) + 2 * (m & 3) + h;
+          const uint32_t q = (en < 8) ? u + 512 * en : u + 512 * (en - 8) + 4096;
+          const uint32_t P = 4096 + (q & 4095u);
+          const bool ob = (C[4096 + 4 * (P >> 5) + 2] >> (P & 31)) & 1u;
+          const uint32_t sp = perm_src(C, q) & 8191u;
+          const bool need = live[P] && !(en >= 8 && ob);
+          if (need) atomicOr(&need_bits[sp >> 5], 1u << (sp & 31));
+          const uint32_t entry = sw(sp) | ((uint32_t)need << 15) |
+                                 ((en == 0 && !deep) ? (1u << 13) : 0u);
+          w |= entry << (16 * h);
+        }
+        D[4 * ((m >> 2) * BT + t) + (m & 3)] = w;
+      }
+      uint32_t A = 0, B = 0;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const uint32_t p = owned_pos(u, i);
+        if (i == 15 && u < 16) continue;
+        const uint32_t *F = C + 4096 + 4 * (p >> 5);
+        A |= ((F[0] >> (p & 31)) & 1u) << i;
+        A |= ((F[1] >> (p & 31)) & 1u) << (16 + i);
+        B |= ((F[2] >> (p & 31)) & 1u) << i;
+        // threads t >= 8: owned position i read from outside its stage
+        if (t >= 8) B |= ((ext_bits[p >> 5] >> (p & 31)) & 1u) << (16 + i);
+      }
+      if (t < 8) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const uint32_t len = 8u >> m;
+          if (t >= len) continue;
+          const uint32_t p = len + t;
+          const uint32_t *F = C + 4096 + 4 * (p >> 5);
+          B |= ((F[0] >> (p & 31)) & 1u) << (16 + m);
+          B |= ((F[1] >> (p & 31)) & 1u) << (20 + m);
+          B |= ((F[2] >> (p & 31)) & 1u) << (24 + m);
+        }
+      }
+      D[4096 + 2 * t] = A;
+      D[4096 + 2 * t + 1] = B;
+      __syncthreads();  // need_bits complete; ext_bits and live free
+    }
     // global-read sources: thread t < 256 appends its masked bits round by
     // round, walking each mask from the lowest set bit; the first appended
     // bit ends up most significant, i.e. at position 32t + total - 1
-    // (csrc/kernel_v1_impl.cuh:87-154).  Unfilled positions get all ones.
+    // (csrc/kernel_v1_impl.cuh:87-154).  Positions no needed stage-0 gather
+    // reads are marked GR_SKIP, unfilled needed ones GR_EMPTY.
     if (t < 256) {
       const uint32_t *gr = src + off + 256;
       uint32_t *G = gr_sources + pid * 8192 + 32 * t;
@@ -901,57 +1034,18 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
           ++i;
         }
       }
-      for (uint32_t k = total; k < 32; ++k) G[k] = 0xffffffffu;
+      for (uint32_t k = total; k < 32; ++k) G[k] = GR_EMPTY;
+      const uint32_t nb = need_bits[t];  // positions 32t .. 32t+31
+      for (uint32_t k = 0; k < 32; ++k)
+        if (!((nb >> k) & 1u)) G[k] = GR_SKIP;
     }
-    const uint32_t *ch = src + off + 256 + 512 * (size_t)R;
-    uint32_t *dch = dst + off + 256 + 512 * (size_t)R;
-    for (uint32_t ci = 0; ci < ns + 2; ++ci) {
+    for (uint32_t ci = ns; ci < ns + 2; ++ci) {
       const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
       uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
-      if (ci < ns) {
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-          // plane m>>2, word m&3: entries 8*(m>>2) + 2*(m&3) + {0, 1}; entry
-          // k < 8 is input a of position 4096+u+512k (source q = u+512k),
-          // entry 8+k its input b (q + 4096)
-          uint32_t w = 0;
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const uint32_t en = 8 * (m >> 2) + 2 * (m & 3) + h;
-            const uint32_t q = (en < 8) ? u + 512 * en : u + 512 * (en - 8) + 4096;
-            w |= sw(perm_src(C, q)) << (16 * h);
-          }
-          D[4 * ((m >> 2) * BT + t) + (m & 3)] = w;
-        }
-        uint32_t A = 0, B = 0;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const uint32_t p = owned_pos(u, i);
-          if (i == 15 && u < 16) continue;
-          const uint32_t *F = C + 4096 + 4 * (p >> 5);
-          A |= ((F[0] >> (p & 31)) & 1u) << i;
-          A |= ((F[1] >> (p & 31)) & 1u) << (16 + i);
-          B |= ((F[2] >> (p & 31)) & 1u) << i;
-        }
-        if (t < 8) {
-#pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            const uint32_t len = 8u >> m;
-            if (t >= len) continue;
-            const uint32_t p = len + t;
-            const uint32_t *F = C + 4096 + 4 * (p >> 5);
-            B |= ((F[0] >> (p & 31)) & 1u) << (16 + m);
-            B |= ((F[1] >> (p & 31)) & 1u) << (20 + m);
-            B |= ((F[2] >> (p & 31)) & 1u) << (24 + m);
-          }
-        }
-        D[4096 + 2 * t] = A;
-        D[4096 + 2 * t + 1] = B;
-      } else {
-        for (uint32_t q2 = t; q2 < 4096; q2 += BT)
-          D[q2] = perm_src(C, 2 * q2) | (perm_src(C, 2 * q2 + 1) << 16);
-      }
+      for (uint32_t q2 = t; q2 < 4096; q2 += BT)
+        D[q2] = perm_src(C, 2 * q2) | (perm_src(C, 2 * q2 + 1) << 16);
     }
+    __syncthreads();  // need_bits read before the next partition clears it
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
     ++pid;
     if (is_last) break;

@@ -28,7 +28,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 def measure(design, split_every, cone, lanes=4, cycles=4, blocks=148, cost_model=None):
     s = design.build_script(num_blocks=blocks, level_split=tuple(range(split_every, 80, split_every)),
                             xprop=True, target_cone=cone, cost_model=cost_model)
-    B = batched.BatchedSim(s, lanes)
+    # single-lane items: the committed model was trained on their timings
+    B = batched.BatchedSim(s, lanes, lanes_per_item=1)
     B.load_state(np.zeros((lanes, B.sig), np.uint32))
     B.reset_sram()
     pc = torch.zeros(s.num_partitions, dtype=torch.int64, device="cuda")
