@@ -140,6 +140,7 @@ struct Shared {
   uint64_t bar[2];
   int ok;
   uint32_t ticket;
+  int dyn;  // items of this major stage come from the ticket counter
 };
 
 // One (block, lane) work item: the block's partition list for one lane word.
@@ -263,7 +264,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         uint32_t A = 0, B = 0, sm = 0;
         // no position below 512 live: levels 5..13 are skipped (uniform:
         // every thread's entry 0 carries it)
-        bool shallow = false;
+        bool shallow = false, flat = false;
         if (ok) {
           const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
           const uint4 pa = P4[t], pb = P4[BT + t];
@@ -271,6 +272,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           A = fl.x;
           B = fl.y;
           shallow = (pa.x >> 13) & 1u;
+          flat = (pa.x >> 29) & 1u;  // only level 1, only positions read from outside
           sm = t < 8 ? 0xffffu : (B >> 16);  // owned positions to store
           // gathers the prepared liveness marks as not needed read nothing
 #define JQ_G(dst, w, h) \
@@ -285,7 +287,17 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           // single buffer: all gathers done before the in-place overwrite
           JQ_FAIL_IF(!ok)
         }
-        if (ok) {
+        if (ok && flat) {
+#define JQ_F1(k)                                                                     \
+  if ((sm >> (k)) & 1u) {                                                            \
+    uint32_t v, x;                                                                   \
+    xand(ga[k].x, ga[k].y, gb[k].x, gb[k].y, mk<k>(A), mk<16 + k>(A), mk<k>(B), v, x); \
+    Sn[4096 + 512 * k + us] = make_uint2(v, x);                                      \
+  }
+          JQ_F1(0) JQ_F1(1) JQ_F1(2) JQ_F1(3) JQ_F1(4) JQ_F1(5) JQ_F1(6) JQ_F1(7)
+#undef JQ_F1
+          if (t == 0) Sn[0] = make_uint2(0, 0);
+        } else if (ok) {
           // level 1 (positions 4096 + u + 512k); owned position i is stored
           // only when read from outside its stage (bit i of sm)
           uint32_t v1[8], x1[8];
@@ -431,7 +443,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         JQ_FAIL_IF(!ok)
         // the item's last commit: take the next work ticket now, so its
         // latency overlaps the commit
-        if (t == 0 && is_last) {
+        if (t == 0 && is_last && sh.dyn) {
           next_ticket = atomicAdd(&g_ticket[P.slot], 1u);
           have_next = true;
         }
@@ -588,7 +600,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         // ---------------- boomerang stage ci
         uint4 v1[8];
         uint32_t A = 0, B = 0, sm = 0;
-        bool shallow = false;  // no position below 512 live
+        bool shallow = false, flat = false;  // no position below 512 / 4096 live
         if (ok) {
           const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
           const uint4 pa = P4[t], pb = P4[BT + t];
@@ -596,19 +608,37 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           A = fl.x;
           B = fl.y;
           shallow = (pa.x >> 13) & 1u;
+          flat = (pa.x >> 29) & 1u;
           sm = t < 8 ? 0xffffu : (B >> 16);
 #define JQ_G(w, h) \
   ((((w) >> (16 * (h) + 15)) & 1u) ? S[((w) >> (16 * (h))) & 0x1fffu] : make_uint4(0, 0, 0, 0))
 #define JQ_L1(k, wa, wb, h) v1[k] = xand2(JQ_G(wa, h), JQ_G(wb, h), mk<k>(A), mk<16 + k>(A), mk<k>(B));
-          JQ_L1(0, pa.x, pb.x, 0) JQ_L1(1, pa.x, pb.x, 1) JQ_L1(2, pa.y, pb.y, 0)
-          JQ_L1(3, pa.y, pb.y, 1) JQ_L1(4, pa.z, pb.z, 0) JQ_L1(5, pa.z, pb.z, 1)
-          JQ_L1(6, pa.w, pb.w, 0) JQ_L1(7, pa.w, pb.w, 1)
+          if (flat) {
+            // only the positions read from outside (warp-uniform skips where
+            // no lane has one)
+#define JQ_F1(k, wa, wb, h) \
+  if ((sm >> (k)) & 1u) JQ_L1(k, wa, wb, h)
+            JQ_F1(0, pa.x, pb.x, 0) JQ_F1(1, pa.x, pb.x, 1) JQ_F1(2, pa.y, pb.y, 0)
+            JQ_F1(3, pa.y, pb.y, 1) JQ_F1(4, pa.z, pb.z, 0) JQ_F1(5, pa.z, pb.z, 1)
+            JQ_F1(6, pa.w, pb.w, 0) JQ_F1(7, pa.w, pb.w, 1)
+#undef JQ_F1
+          } else {
+            JQ_L1(0, pa.x, pb.x, 0) JQ_L1(1, pa.x, pb.x, 1) JQ_L1(2, pa.y, pb.y, 0)
+            JQ_L1(3, pa.y, pb.y, 1) JQ_L1(4, pa.z, pb.z, 0) JQ_L1(5, pa.z, pb.z, 1)
+            JQ_L1(6, pa.w, pb.w, 0) JQ_L1(7, pa.w, pb.w, 1)
+          }
 #undef JQ_L1
 #undef JQ_G
         }
         // single buffer: every gather done before the first overwrite
         JQ_FAIL_IF(!ok)
-        {
+        if (flat) {
+#define JQ_ST1(k) \
+  if ((sm >> (k)) & 1u) S[4096 + 512 * k + us] = v1[k];
+          JQ_ST1(0) JQ_ST1(1) JQ_ST1(2) JQ_ST1(3) JQ_ST1(4) JQ_ST1(5) JQ_ST1(6) JQ_ST1(7)
+#undef JQ_ST1
+          if (t == 0) S[0] = make_uint4(0, 0, 0, 0);
+        } else {
 #define JQ_ST1(k) \
   if (((sm >> (k)) & 1u)) S[4096 + 512 * k + us] = v1[k];
           JQ_ST1(0) JQ_ST1(1) JQ_ST1(2) JQ_ST1(3) JQ_ST1(4) JQ_ST1(5) JQ_ST1(6) JQ_ST1(7)
@@ -731,28 +761,46 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       } else {
         // ---------------- clock-enable permutation and commit, both lane words
         JQ_FAIL_IF(!ok)
-        if (t == 0 && is_last) {
+        if (t == 0 && is_last && sh.dyn) {
           next_ticket = atomicAdd(&g_ticket[P.slot], 1u);
           have_next = true;
         }
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
-        for (uint32_t q = t; q < nq; q += BT) {
-          const uint4 src = WO[perm_lin(C, q)];
-          const uint4 fl = F4[q >> 5];
-          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q), dinv = bitmask(fl.z, q);
-          const uint4 me = WO[q];
-          const size_t sg = (size_t)io_off * 32 + q;
-          const uint32_t old0 = ldcg(in + base0 + sg), old1 = ldcg(in + base1 + sg);
-          const uint32_t oldx0 = is_x ? ldcg(in + xsig + base0 + sg) : 0u;
-          const uint32_t oldx1 = is_x ? ldcg(in + xsig + base1 + sg) : 0u;
-          const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
-          out[base0 + sg] = (old0 & ~cp0) | ((me.x ^ dinv) & cp0);
-          out[base1 + sg] = (old1 & ~cp1) | ((me.z ^ dinv) & cp1);
-          if (is_x) {
-            const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
-            out[xsig + base0 + sg] = (oldx0 & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0;
-            out[xsig + base1 + sg] = (oldx1 & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1;
+        // the old words of up to 4 q per thread are loaded before any store,
+        // so their latencies overlap
+        for (uint32_t q0 = t; q0 < nq; q0 += 2 * BT) {
+          uint32_t o[2][4];  // old v0, v1, x0, x1
+#pragma unroll
+          for (int uu = 0; uu < 2; ++uu) {
+            const uint32_t q = q0 + uu * BT;
+            if (q < nq) {
+              const size_t sg = (size_t)io_off * 32 + q;
+              o[uu][0] = ldcg(in + base0 + sg);
+              o[uu][1] = ldcg(in + base1 + sg);
+              o[uu][2] = is_x ? ldcg(in + xsig + base0 + sg) : 0u;
+              o[uu][3] = is_x ? ldcg(in + xsig + base1 + sg) : 0u;
+            }
+          }
+#pragma unroll
+          for (int uu = 0; uu < 2; ++uu) {
+            const uint32_t q = q0 + uu * BT;
+            if (q < nq) {
+              const uint4 src = WO[perm_lin(C, q)];
+              const uint4 fl = F4[q >> 5];
+              const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q),
+                             dinv = bitmask(fl.z, q);
+              const uint4 me = WO[q];
+              const size_t sg = (size_t)io_off * 32 + q;
+              const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
+              out[base0 + sg] = (o[uu][0] & ~cp0) | ((me.x ^ dinv) & cp0);
+              out[base1 + sg] = (o[uu][1] & ~cp1) | ((me.z ^ dinv) & cp1);
+              if (is_x) {
+                const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
+                out[xsig + base0 + sg] = (o[uu][2] & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0;
+                out[xsig + base1 + sg] = (o[uu][3] & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1;
+              }
+            }
           }
         }
       }
@@ -767,6 +815,34 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
   }
 }
 #undef JQ_FAIL_IF
+
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.L2 [%0];" ::"l"(p));
+}
+
+// L2 prefetch of what the CTA's item of major stage ms reads first, when
+// that stage assigns items statically (at most one per CTA): the global-read
+// source table of its first partition and the head of its script (metadata,
+// global-read section, the first two chunks).  Threads i0 = 0..n-1 share it.
+template <int NL>
+__device__ void prefetch_item_l2(const BatchParams &P, unsigned ms, uint32_t i0, uint32_t n) {
+  const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
+                                     : P.num_blocks;
+  const uint32_t per = P.lanes / NL;
+  if ((size_t)nblk * per > gridDim.x || blockIdx.x >= nblk * per) return;
+  const uint32_t bi = blockIdx.x / per;
+  const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
+  const size_t e = (size_t)ms * P.num_blocks + blk;
+  const uint32_t *script = P.blocks_data + P.blocks_start[e];
+  const uint32_t *gr = P.gr_sources + (size_t)P.part_base[e] * 8192;
+  // the script window ends at the end of the script data
+  const size_t left = P.blocks_start[(size_t)P.num_major_stages * P.num_blocks] - P.blocks_start[e];
+  constexpr uint32_t GR_LINES = 8192 / 32;                  // 128-byte lines
+  constexpr size_t WINDOW = 256 + 512 * 8 + 2 * STAGE_WORDS;
+  const uint32_t script_lines = (uint32_t)((left < WINDOW ? left : WINDOW) / 32);
+  for (uint32_t l = i0; l < GR_LINES + script_lines; l += n)
+    prefetch_l2(l < GR_LINES ? gr + 32 * l : script + 32 * (l - GR_LINES));
+}
 
 // NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
 template <bool DS, int NL>
@@ -819,13 +895,22 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
                                          : P.num_blocks;
       const uint32_t per = P.lanes / NL;  // items per block
       const uint32_t items = nblk * per;
+      // at most one item per CTA: item = CTA index (so the CTA knows its
+      // next item early and can prefetch it); otherwise tickets
+      const bool dyn = items > gridDim.x;
       uint32_t next_ticket = 0;
       bool have_next = false;
+      bool done_static = false;
       for (;;) {
         __syncthreads();
-        if (t == 0) sh.ticket = have_next ? next_ticket : atomicAdd(&g_ticket[P.slot], 1u);
+        if (t == 0) {
+          sh.dyn = dyn;
+          sh.ticket = !dyn ? (done_static ? items : blockIdx.x)
+                           : have_next ? next_ticket : atomicAdd(&g_ticket[P.slot], 1u);
+        }
         __syncthreads();
         have_next = false;
+        done_static = true;
         const uint32_t tk = sh.ticket;
         if (tk >= items) break;
         const uint32_t bi = tk / per, lane = tk % per;
@@ -843,8 +928,14 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
           return;
         }
       }
-      // last arriver re-arms the ticket counter inside the barrier
+      // last arriver re-arms the ticket counter inside the barrier; while
+      // thread 0 waits, warps 1.. prefetch this CTA's next item into L2
       __syncthreads();
+      if (t >= 32) {
+        const unsigned ms2 = ms + 1 < P.num_major_stages ? ms + 1 : 0;
+        if (ms + 1 < P.num_major_stages || c + 1 < P.num_cycles)
+          prefetch_item_l2<NL>(P, ms2, t - 32, BT - 32);
+      }
       if (t == 0) {
         unsigned gen = ld_acquire(&g_bar_gen[P.slot]);
         __threadfence();
@@ -907,7 +998,9 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 // source entries are 13-bit tree addresses; their top bits carry
 //   bit 15  the gather is needed (otherwise the kernel reads nothing and
 //           uses 0, which only feeds dead positions or an ob-forced input);
-//   bit 13  of entry 0: no position below 512 is live (levels 5..13 skipped).
+//   bit 13  of entry 0: no position below 512 is live (levels 5..13 skipped);
+//           of entry 1: no position below 4096 is live (only level 1 runs,
+//           and only for positions read from outside).
 // Bits 16+i of the second flag word of threads t >= 8 mark owned position i
 // as read from outside its stage; only those are stored (threads t < 8 hold
 // the warp-0 flags there and store all their positions).
@@ -960,6 +1053,9 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         __syncthreads();
       }
       const int deep = __syncthreads_or(t > 0 && live[t]);  // BT = 512
+      int upper = 0;  // any live position in [512, 4096) (levels 2..4)
+      for (uint32_t c = 512 + t; c < 4096; c += BT) upper |= live[c];
+      const int flat = !deep && !__syncthreads_or(upper);  // level 1 only
       for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;
       __syncthreads();
 #pragma unroll
@@ -978,7 +1074,8 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
           const bool need = live[P] && !(en >= 8 && ob);
           if (need) atomicOr(&need_bits[sp >> 5], 1u << (sp & 31));
           const uint32_t entry = sw(sp) | ((uint32_t)need << 15) |
-                                 ((en == 0 && !deep) ? (1u << 13) : 0u);
+                                 ((en == 0 && !deep) ? (1u << 13) : 0u) |
+                                 ((en == 1 && flat) ? (1u << 13) : 0u);
           w |= entry << (16 * h);
         }
         D[4 * ((m >> 2) * BT + t) + (m & 3)] = w;

@@ -152,6 +152,7 @@ class Design:
 
     def _load_info(self):
         lib = _lib()
+        self._free = lib.jqf_free_design  # held for __del__ at interpreter exit
         info = _DesignInfo()
         lib.jqf_design_info(self._h, ctypes.byref(info))
         self.num_pins = info.num_pins
@@ -164,8 +165,9 @@ class Design:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib().jqf_free_design(h)
+        free = getattr(self, "_free", None)
+        if h and free is not None:
+            free(h)
             self._h = None
 
     def array(self, which):
