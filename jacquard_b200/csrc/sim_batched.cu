@@ -147,11 +147,13 @@ struct Shared {
 // Tree state and writeouts hold (value, X) pairs so one shared-memory access
 // moves both.  The script is in the prepared layout (jq_batched_prepare):
 //   boomerang chunk: words [0, 4096) two uint4 planes [2][512 threads], the
-//     thread's 16 gather sources (level-1 inputs a then b, already swizzled);
+//     thread's 16 gather sources (level-1 inputs a then b, already swizzled,
+//     with the liveness bits of the prepare step);
 //     words [4096, 5120) one uint2 per thread: xa bits 0..15 | xb bits 16..31,
-//     ob bits 0..15 of its 16 owned positions, and for warp-0 threads t < 8
-//     the flags of tree positions 8+t, 4+t, 2+t, 1+t (levels 10..13) at
-//     bits 16+m (xa), 20+m (xb), 24+m (ob) of the second word;
+//     ob bits 0..15 of its 16 owned positions, then bits 16..31 the store
+//     mask of those positions, except that in deep stages warp-0 threads
+//     t < 8 hold there the flags of tree positions 8+t, 4+t, 2+t, 1+t
+//     (levels 10..13) at bits 16+m (xa), 20+m (xb), 24+m (ob);
 //   SRAM/duplicate and clock-enable chunks: shuffle entries in q order,
 //     flags unchanged.
 // With `ds` the tree state is double-buffered (stage ci reads buffer ci&1 and
@@ -232,6 +234,14 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     const uint32_t lane_i = t & 31, warp_i = t >> 5;
     const uint32_t u = residue(t);
     const uint32_t us = sw(u);
+    // writeout hook (stage << 8 | 32-position group) of slot warp_i + 16 *
+    // lane_i (lanes 0..15; num_ios <= 256), all ones when there is none
+    uint32_t my_hook = 0xffffffffu;
+    if (lane_i < 16 && warp_i + 16 * lane_i < num_ios) {
+      const uint32_t slot = warp_i + 16 * lane_i;
+      const uint32_t hw = sh.meta[128 + slot / 2];
+      my_hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+    }
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
       const uint32_t b = ci & 1;
       uint32_t *C = chunks + b * STAGE_WORDS;
@@ -273,7 +283,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           B = fl.y;
           shallow = (pa.x >> 13) & 1u;
           flat = (pa.x >> 29) & 1u;  // only level 1, only positions read from outside
-          sm = t < 8 ? 0xffffu : (B >> 16);  // owned positions to store
+          sm = t < 8 && !shallow ? 0xffffu : (B >> 16);  // owned positions to store
           // gathers the prepared liveness marks as not needed read nothing
 #define JQ_G(dst, w, h) \
   dst = (((w) >> (16 * (h) + 15)) & 1u) ? Sp[((w) >> (16 * (h))) & 0x1fffu] : make_uint2(0, 0);
@@ -375,11 +385,12 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           }
           __syncthreads();
         }
-        // writeout hooks of this stage: warp w scans slots w, w+16, ...
-        for (uint32_t slot = warp_i; slot < num_ios; slot += BT / 32) {
-          const uint32_t hw = sh.meta[128 + slot / 2];
-          const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
-          if ((hook >> 8) == ci) WO[slot * 32 + lane_i] = Sn[sw((hook & 255u) * 32 + lane_i)];
+        // writeout hooks of this stage: warp w copies those of slots w,
+        // w+16, ... (lane j holds slot w+16j's hook)
+        for (uint32_t hm = __ballot_sync(0xffffffffu, (my_hook >> 8) == ci); hm; hm &= hm - 1) {
+          const uint32_t j = __ffs(hm) - 1;
+          const uint32_t g = __shfl_sync(0xffffffffu, my_hook, j) & 255u;
+          WO[(warp_i + 16 * j) * 32 + lane_i] = Sn[sw(g * 32 + lane_i)];
         }
       } else if (has_sram && ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports
@@ -577,6 +588,14 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     const uint32_t lane_i = t & 31, warp_i = t >> 5;
     const uint32_t u = residue(t);
     const uint32_t us = sw(u);
+    // writeout hook (stage << 8 | 32-position group) of slot warp_i + 16 *
+    // lane_i (lanes 0..15; num_ios <= 256), all ones when there is none
+    uint32_t my_hook = 0xffffffffu;
+    if (lane_i < 16 && warp_i + 16 * lane_i < num_ios) {
+      const uint32_t slot = warp_i + 16 * lane_i;
+      const uint32_t hw = sh.meta[128 + slot / 2];
+      my_hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+    }
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
       const uint32_t b = ci & 1;
       uint32_t *C = chunks + b * STAGE_WORDS;
@@ -609,7 +628,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           B = fl.y;
           shallow = (pa.x >> 13) & 1u;
           flat = (pa.x >> 29) & 1u;
-          sm = t < 8 ? 0xffffu : (B >> 16);
+          sm = t < 8 && !shallow ? 0xffffu : (B >> 16);
 #define JQ_G(w, h) \
   ((((w) >> (16 * (h) + 15)) & 1u) ? S[((w) >> (16 * (h))) & 0x1fffu] : make_uint4(0, 0, 0, 0))
 #define JQ_L1(k, wa, wb, h) v1[k] = xand2(JQ_G(wa, h), JQ_G(wb, h), mk<k>(A), mk<16 + k>(A), mk<k>(B));
@@ -692,10 +711,10 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           }
           __syncthreads();
         }
-        for (uint32_t slot = warp_i; slot < num_ios; slot += BT / 32) {
-          const uint32_t hw = sh.meta[128 + slot / 2];
-          const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
-          if ((hook >> 8) == ci) WO[slot * 32 + lane_i] = S[sw((hook & 255u) * 32 + lane_i)];
+        for (uint32_t hm = __ballot_sync(0xffffffffu, (my_hook >> 8) == ci); hm; hm &= hm - 1) {
+          const uint32_t j = __ffs(hm) - 1;
+          const uint32_t g = __shfl_sync(0xffffffffu, my_hook, j) & 255u;
+          WO[(warp_i + 16 * j) * 32 + lane_i] = S[sw(g * 32 + lane_i)];
         }
       } else if (has_sram && ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports
@@ -1001,9 +1020,9 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 //   bit 13  of entry 0: no position below 512 is live (levels 5..13 skipped);
 //           of entry 1: no position below 4096 is live (only level 1 runs,
 //           and only for positions read from outside).
-// Bits 16+i of the second flag word of threads t >= 8 mark owned position i
-// as read from outside its stage; only those are stored (threads t < 8 hold
-// the warp-0 flags there and store all their positions).
+// Bits 16+i of the second flag word mark owned position i as read from
+// outside its stage; only those are stored.  In deep stages threads t < 8
+// hold the warp-0 flags there instead and store all their positions.
 // Unneeded global-read positions get source 0xfffffffe (neither loaded nor
 // stored).  Dead positions are neither stored nor read, so the state they
 // leave in shared memory is never observed.
@@ -1089,10 +1108,11 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         A |= ((F[0] >> (p & 31)) & 1u) << i;
         A |= ((F[1] >> (p & 31)) & 1u) << (16 + i);
         B |= ((F[2] >> (p & 31)) & 1u) << i;
-        // threads t >= 8: owned position i read from outside its stage
-        if (t >= 8) B |= ((ext_bits[p >> 5] >> (p & 31)) & 1u) << (16 + i);
+        // owned position i read from outside its stage (threads t < 8 of
+        // deep stages hold the warp-0 flags there instead)
+        if (t >= 8 || !deep) B |= ((ext_bits[p >> 5] >> (p & 31)) & 1u) << (16 + i);
       }
-      if (t < 8) {
+      if (t < 8 && deep) {
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const uint32_t len = 8u >> m;
