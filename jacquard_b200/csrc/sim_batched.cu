@@ -841,10 +841,14 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
 
 // L2 prefetch of what the CTA's item of major stage ms reads first, when
 // that stage assigns items statically (at most one per CTA): the global-read
-// source table of its first partition and the head of its script (metadata,
-// global-read section, the first two chunks).  Threads i0 = 0..n-1 share it.
+// source table of its first partition, the head of its script (metadata,
+// global-read section, the first two chunks) and the previous-cycle state
+// rows `prev` its commit reads (a partition commits to the words it wrote a
+// cycle earlier, long evicted by then).  Threads i0 = 0..n-1 share it;
+// prefetches are hints and change no data.
 template <int NL>
-__device__ void prefetch_item_l2(const BatchParams &P, unsigned ms, uint32_t i0, uint32_t n) {
+__device__ void prefetch_item_l2(const BatchParams &P, unsigned ms, const uint32_t *prev,
+                                 uint32_t i0, uint32_t n) {
   const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
                                      : P.num_blocks;
   const uint32_t per = P.lanes / NL;
@@ -861,6 +865,19 @@ __device__ void prefetch_item_l2(const BatchParams &P, unsigned ms, uint32_t i0,
   const uint32_t script_lines = (uint32_t)((left < WINDOW ? left : WINDOW) / 32);
   for (uint32_t l = i0; l < GR_LINES + script_lines; l += n)
     prefetch_l2(l < GR_LINES ? gr + 32 * l : script + 32 * (l - GR_LINES));
+  // commit rows of the first partition: [io_off*32, +num_ios*32) of each
+  // lane word of the item and of their X planes
+  const uint32_t ns = script[0], num_ios = script[2], io_off = script[3];
+  if (ns == 0) return;
+  const bool is_x = script[8] != 0;
+  const size_t xsig = (size_t)script[9] * 32;
+  const size_t b0 = (size_t)(NL * (blockIdx.x % per)) * P.sig_per_snap + (size_t)io_off * 32;
+  const uint32_t rows = NL * (is_x ? 2 : 1);
+  for (uint32_t l = i0; l < rows * num_ios; l += n) {
+    const uint32_t r = l / num_ios, k = l % num_ios;  // row (lane word, plane), 128-byte line
+    const size_t base = b0 + (size_t)(is_x ? r >> 1 : r) * P.sig_per_snap + (is_x && (r & 1) ? xsig : 0);
+    prefetch_l2(prev + base + 32 * (size_t)k);
+  }
 }
 
 // NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
@@ -952,8 +969,10 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       __syncthreads();
       if (t >= 32) {
         const unsigned ms2 = ms + 1 < P.num_major_stages ? ms + 1 : 0;
+        // the next stage's previous-cycle snapshot: `in`, or at the end of
+        // the cycle this cycle's `out`
         if (ms + 1 < P.num_major_stages || c + 1 < P.num_cycles)
-          prefetch_item_l2<NL>(P, ms2, t - 32, BT - 32);
+          prefetch_item_l2<NL>(P, ms2, ms + 1 < P.num_major_stages ? in : out, t - 32, BT - 32);
       }
       if (t == 0) {
         unsigned gen = ld_acquire(&g_bar_gen[P.slot]);
