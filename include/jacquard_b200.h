@@ -110,10 +110,17 @@ int jq_max_blocks(int device, size_t *max_blocks);
 
 /* ------------------------------------------------------------------------ */
 /* Bit-lane batched interpreter: 32*lanes independent stimulus streams run the
- * same script in one persistent launch.  State is lane-major: snapshot word
- * [l * signals_per_snapshot + signal] holds one signal (a bit position of the
- * reference layout, word*32+bit, X plane at metadata word 9 * 32) for
- * streams 32l..32l+31.  Two snapshot buffers ping-pong: cycle c reads state_a when c
+ * same script in one persistent launch.  A lane word holds one signal (a bit
+ * position of the reference layout, word*32+bit, X plane at metadata word
+ * 9 * 32) for streams 32l..32l+31.  The state buffers interleave lane pairs
+ * (jq_batched_state_words words; lanes rounded up to even):
+ *   x_interleaved = 1 (V = signals_per_snapshot / 2 value signals, signal
+ *     V + s the X of s): word ((l >> 1) * V + s mod V) * 4 + 2 * (l & 1) +
+ *     (s >= V), i.e. (value, X) of the even lane, then of the odd lane;
+ *   x_interleaved = 0: word ((l >> 1) * signals + s) * 2 + (l & 1).
+ * jq_batched_pack_state / jq_batched_unpack_state convert from / to the
+ * lane-major form [l][signal] that `stimulus`, `wave` and `record` use.
+ * Two snapshot buffers ping-pong: cycle c reads state_a when c
  * is even (state_b when odd) and writes the other; after num_cycles cycles the
  * final state is in state_a if num_cycles is even, else state_b.  Both buffers
  * must start with snapshot 0 (values, X template).  Words that no partition
@@ -164,6 +171,12 @@ typedef struct {
                                   of a lane pair fits the writeouts, else 1),
                                   1, or 2 (JQ_ERR_INVALID_ARG when it does not
                                   fit or lanes is odd) */
+  int32_t x_interleaved;       /* state layout (below): 1 when signals
+                                  [S/2, S) are the X planes of [0, S/2)
+                                  (S = signals_per_snapshot; required when any
+                                  partition is X-capable, and then every such
+                                  partition's X offset, metadata word 9, is
+                                  S/64 words), 0 for scripts without X */
 } jq_batch_args;
 
 /* Prepares a script (FlattenedScriptV1, device arrays) for the batched
@@ -184,6 +197,14 @@ int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
                        size_t num_partitions, uint32_t *out, uint32_t *part_base,
                        uint32_t *gr_sources, void *stream);
 int jq_simulate_batched(const jq_batch_args *a);
+/* Words of one batched state buffer. */
+size_t jq_batched_state_words(uint32_t lanes, size_t signals);
+/* Lane-major [lanes][signals] (device) <-> batched state layout (device),
+ * asynchronous on `stream`. */
+int jq_batched_pack_state(const uint32_t *lane_major, uint32_t lanes, size_t signals,
+                          int32_t x_interleaved, uint32_t *state, void *stream);
+int jq_batched_unpack_state(const uint32_t *state, uint32_t lanes, size_t signals,
+                            int32_t x_interleaved, uint32_t *lane_major, void *stream);
 /* Synchronizes `stream`; JQ_OK or the kernel's recorded error. */
 int jq_batched_status(void *stream);
 int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks);

@@ -28,7 +28,7 @@ class BatchArgs(ctypes.Structure):
                 ("part_cycles", vp), ("part_base", vp), ("gr_sources", vp),
                 ("grid", ctypes.c_size_t),
                 ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp),
-                ("lanes_per_item", ctypes.c_uint32)]
+                ("lanes_per_item", ctypes.c_uint32), ("x_interleaved", ctypes.c_int32)]
 
 
 def lib():
@@ -45,6 +45,11 @@ def lib():
         L.jq_batched_prepare.restype = ctypes.c_int
         L.jq_batched_prepare.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
                                          ctypes.c_size_t, vp, vp, vp, vp]
+        L.jq_batched_state_words.restype = ctypes.c_size_t
+        L.jq_batched_state_words.argtypes = [ctypes.c_uint32, ctypes.c_size_t]
+        for fn in (L.jq_batched_pack_state, L.jq_batched_unpack_state):
+            fn.restype = ctypes.c_int
+            fn.argtypes = [vp, ctypes.c_uint32, ctypes.c_size_t, ctypes.c_int32, vp, vp]
         L._jq_batched_typed = True
     return L
 
@@ -120,6 +125,24 @@ def block_lists(script):
     return np.asarray(lst if lst else [0], np.uint32), np.asarray(start, np.uint32)
 
 
+def check_x_offsets(script, value_words):
+    """Every X-capable partition's X offset (metadata word 9) must be
+    value_words: the batched kernel takes a signal's X plane from the quad
+    layout, not from the offset."""
+    bd = np.asarray(script.blocks_data, dtype=np.uint32)
+    starts = np.asarray(script.blocks_start, dtype=np.int64)
+    for off in starts[:-1].tolist():
+        while True:
+            ns = int(bd[off])
+            if ns == 0:
+                break
+            if bd[off + 8] and int(bd[off + 9]) != value_words:
+                raise ValueError(f"X offset {int(bd[off + 9])} != {value_words} value words")
+            if bd[off + 1]:
+                break
+            off += 256 + 512 * int(bd[off + 6]) + 5120 * (ns + 2)
+
+
 class BatchedSim:
     """Script + buffers on the device for `lanes` lane words (32*lanes streams)."""
 
@@ -152,6 +175,11 @@ class BatchedSim:
         self.eff = getattr(script, "effective_words", None) or \
             script.reg_io_state_size * (2 if script.xprop_enabled else 1)
         self.sig = self.eff * 32
+        # X-capable scripts run in the quad layout: signals [sig/2, sig) are
+        # the X planes of [0, sig/2), which every X partition's offset must say
+        self.x_interleaved = 1 if script.xprop_enabled else 0
+        if self.x_interleaved:
+            check_x_offsets(script, self.eff // 2)
         regions = getattr(script, "input_regions", None)
         if regions is None:
             self.in_sigs = input_words(script) * 32
@@ -168,7 +196,8 @@ class BatchedSim:
         self.block_list_start = torch.from_numpy(bls.view(np.int32)).to(self.device)
         self.sram_words = max(1, script.sram_storage_size)
         n_streams = 32 * lanes
-        self.state_a = torch.zeros(self.sig * lanes, dtype=torch.int32, device=self.device)
+        self.state_a = torch.zeros(L.jq_batched_state_words(lanes, self.sig), dtype=torch.int32,
+                                   device=self.device)
         self.state_b = torch.zeros_like(self.state_a)
         self.sram = torch.zeros(n_streams * self.sram_words, dtype=torch.int32, device=self.device)
         self.sram_x = torch.full_like(self.sram, -1)
@@ -181,11 +210,18 @@ class BatchedSim:
         # lanes is even and they fit), 1 or 2 forces one
         self.lanes_per_item = lanes_per_item
 
+    def _convert(self, fn, src, dst):
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        rc = fn(src.data_ptr(), self.lanes, self.sig, self.x_interleaved, dst.data_ptr(), st)
+        if rc:
+            raise RuntimeError("batched state conversion: " + sim.lib().jq_strerror(rc).decode())
+
     def load_state(self, snap0):
-        """snap0: (lanes, sig) u32 batched snapshot 0 (values + X template)."""
+        """snap0: (lanes, sig) u32 lane-major snapshot 0 (values + X template)."""
         t = torch.from_numpy(np.ascontiguousarray(snap0, np.uint32).reshape(-1).view(np.int32)).to(self.device)
-        self.state_a.copy_(t)
-        self.state_b.copy_(t)
+        assert t.numel() == self.lanes * self.sig
+        self._convert(lib().jq_batched_pack_state, t, self.state_a)
+        self.state_b.copy_(self.state_a)
 
     def reset_sram(self, x=True):
         self.sram.zero_()
@@ -223,7 +259,7 @@ class BatchedSim:
                       self.part_base_dev.data_ptr(), self.gr_sources.data_ptr(),
                       self.grid, 0,
                       stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream,
-                      self.lanes_per_item)
+                      self.lanes_per_item, self.x_interleaved)
         rc = L.jq_simulate_batched(ctypes.byref(a))
         if rc:
             raise RuntimeError("jq_simulate_batched: " + sim.lib().jq_strerror(rc).decode())
@@ -233,7 +269,11 @@ class BatchedSim:
         return lib().jq_batched_status(s)
 
     def final_state(self, cycles):
-        return self.state_a if cycles % 2 == 0 else self.state_b
+        """Lane-major (lanes * sig) copy of the state after `cycles` cycles."""
+        src = self.state_a if cycles % 2 == 0 else self.state_b
+        out = torch.empty(self.lanes * self.sig, dtype=torch.int32, device=self.device)
+        self._convert(lib().jq_batched_unpack_state, src, out)
+        return out
 
 
 class CombinedScript:
@@ -241,10 +281,11 @@ class CombinedScript:
     single persistent launch runs them all (work items of every design share
     the CTAs; designs with fewer major stages leave empty blocks).
 
+    The combined state holds every design's value words, then every design's
+    X words in the same order (the batched quad layout needs one X offset).
     Relocation only shifts absolute offsets: IO offset (metadata word 3), SRAM
-    offset (word 5) and global-read word indices move by the design's state /
-    SRAM base; the X offset (word 9) stays the design's own value-plane size
-    because each design keeps its [values | X] pair contiguous."""
+    offset (word 5) and global-read word indices move by the design's value /
+    SRAM base, and the X offset (word 9) becomes the total value words."""
 
     def __init__(self, scripts):
         self.parts = scripts
@@ -259,12 +300,13 @@ class CombinedScript:
             self.state_base.append(sb)
             self.sram_base.append(srb)
             self.block_base.append(bb)
-            sb += 2 * s.reg_io_state_size
+            sb += s.reg_io_state_size
             srb += s.sram_storage_size
             bb += s.num_blocks
-        self.effective_words = sb
+        self.value_words = sb
+        self.effective_words = 2 * sb
         self.sram_storage_size = srb
-        self.reg_io_state_size = sb // 2  # not used for layout (effective_words is)
+        self.reg_io_state_size = sb
         data, starts, sbp = [], [], []
         pos = 0
         dummy = np.zeros(256, np.uint32)
@@ -289,6 +331,8 @@ class CombinedScript:
                         R = int(blk[off + 6])
                         blk[off + 3] += self.state_base[d]
                         blk[off + 5] += self.sram_base[d]
+                        if blk[off + 8]:
+                            blk[off + 9] = self.value_words
                         g = blk[off + 256: off + 256 + 512 * R].reshape(-1, 2)
                         nz = g[:, 1] != 0
                         hi_bit = g[:, 0] & np.uint32(0x80000000)
@@ -319,5 +363,23 @@ class CombinedScript:
         return int(self.blocks_start[-1])
 
     def signal(self, d, sig):
-        """Combined signal index of design d's signal `sig`."""
-        return self.state_base[d] * 32 + sig
+        """Combined signal index of design d's signal `sig` (its own layout:
+        values, then X at reg_io_state_size * 32)."""
+        n = self.parts[d].reg_io_state_size * 32
+        if sig < n:
+            return self.state_base[d] * 32 + sig
+        return (self.value_words + self.state_base[d]) * 32 + sig - n
+
+    def combine_states(self, states):
+        """Per-design lane-major states (..., 2 * rio_d * 32) -> the combined
+        lane-major state (..., 2 * value_words * 32)."""
+        vals = [st[..., :s.reg_io_state_size * 32] for st, s in zip(states, self.parts)]
+        xs = [st[..., s.reg_io_state_size * 32:] for st, s in zip(states, self.parts)]
+        return np.concatenate(vals + xs, axis=-1)
+
+    def design_state(self, d, state):
+        """Design d's lane-major state (values, then X) out of a combined one."""
+        n = self.parts[d].reg_io_state_size * 32
+        lo = self.state_base[d] * 32
+        xlo = (self.value_words + self.state_base[d]) * 32
+        return np.concatenate([state[..., lo:lo + n], state[..., xlo:xlo + n]], axis=-1)

@@ -45,6 +45,8 @@ struct BatchParams {
   size_t sram_words;
   size_t num_cycles;
   size_t sig_per_snap;      // effective words * 32
+  int xhalf;                // quad layout: signals [V, 2V) are the X of [0, V)
+  size_t vsig;              // V: value signals (sig_per_snap / 2 with xhalf)
   uint32_t *state_a, *state_b;  // ping-pong snapshots, lane-major
   const uint32_t *stim;     // [cycle+1][lanes][input_sigs] input values, or null
   size_t input_sigs;        // stimulus signals per lane per cycle
@@ -135,6 +137,25 @@ __host__ __device__ __forceinline__ uint32_t owned_pos(uint32_t u, int i) {
                         : i < 14 ? 1024 + u + 512 * (i - 12) : i == 14 ? 512 + u : u;
 }
 
+// Word of (lane l, signal s) in the batched state.  Lane pairs are
+// interleaved so the two lane words of a pair (and, with X, their X words)
+// share one 8- or 16-byte access:
+//   quad layout (xhalf, signals [V, 2V) the X of [0, V)):
+//     ((l >> 1) * V + s mod V) * 4 + 2 * (l & 1) + (s >= V)
+//     i.e. (v_even, x_even, v_odd, x_odd) per lane pair and value signal;
+//   pair layout: ((l >> 1) * sig + s) * 2 + (l & 1).
+__host__ __device__ __forceinline__ size_t phys(int xhalf, size_t vsig, size_t sig, uint32_t l,
+                                                size_t s) {
+  if (xhalf) {
+    const bool x = s >= vsig;
+    return ((((size_t)(l >> 1)) * vsig + (x ? s - vsig : s)) << 2) + 2 * (l & 1) + (x ? 1 : 0);
+  }
+  return ((((size_t)(l >> 1)) * sig + s) << 1) + (l & 1);
+}
+__device__ __forceinline__ size_t phys(const BatchParams &P, uint32_t l, size_t s) {
+  return phys(P.xhalf, P.vsig, P.sig_per_snap, l, s);
+}
+
 struct Shared {
   uint32_t meta[256];
   uint64_t bar[2];
@@ -164,7 +185,12 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
                          const uint32_t *in, uint32_t *out, uint32_t lane, uint32_t pid0,
                          bool &failed, uint32_t &next_ticket, bool &have_next) {
   const int t = threadIdx.x;
-  const size_t lane_base = (size_t)lane * P.sig_per_snap;
+  // the lane's words: with xhalf (v, x) pairs at 4 * (pair * V + s) + 2 * odd
+  // (X-capable partitions always run in the quad layout), else values at
+  // 2 * (pair * sig + s) + odd
+  const size_t lane_base = P.xhalf ? (((size_t)(lane >> 1) * P.vsig) << 2) + 2 * (lane & 1)
+                                   : (((size_t)(lane >> 1) * P.sig_per_snap) << 1) + (lane & 1);
+  const uint32_t sig_shift = P.xhalf ? 2 : 1;
   constexpr bool ds = DS;
   uint2 *const Sb0 = S;
   uint2 *const Sb1 = ds ? S + 8192 : S;
@@ -188,7 +214,6 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     const uint32_t num_srams = sh.meta[4], sram_off = sh.meta[5], R = sh.meta[6];
     const uint32_t num_dup = sh.meta[7];
     const bool is_x = sh.meta[8] != 0;
-    const uint32_t xsig = sh.meta[9] * 32u;
     const uint32_t *gr = script + off + 256;
     const uint32_t *ch0 = gr + 512 * (size_t)R;
     // chunk sequence: the ns boomerang stages, the SRAM/duplicate chunk
@@ -215,9 +240,14 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         vx[k] = 0;
         if (e[k] < GR_SKIP) {
           const uint32_t *base = (e[k] >> 31) ? out : in;
-          const size_t sg = lane_base + (e[k] & 0x7fffffffu);
-          v[k] = ldcg(base + sg);
-          if (is_x) vx[k] = ldcg(base + xsig + sg);
+          const size_t w = lane_base + ((size_t)(e[k] & 0x7fffffffu) << sig_shift);
+          if (P.xhalf) {
+            const uint2 q = __ldcg(reinterpret_cast<const uint2 *>(base + w));
+            v[k] = q.x;
+            vx[k] = is_x ? q.y : 0u;
+          } else {
+            v[k] = ldcg(base + w);
+          }
         }
       }
 #pragma unroll
@@ -476,19 +506,27 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
               cpx[uu] = is_x ? (src.y & ~set0) : 0u;
               wv[uu] = me.x ^ dinv;
               wx[uu] = me.y;
-              sg[uu] = lane_base + (size_t)io_off * 32 + q;
-              old[uu] = ldcg(in + sg[uu]);
-              oldx[uu] = is_x ? ldcg(in + xsig + sg[uu]) : 0u;
+              sg[uu] = lane_base + (((size_t)io_off * 32 + q) << sig_shift);
+              if (is_x) {  // quad layout: (v, x) adjacent
+                const uint2 o = __ldcg(reinterpret_cast<const uint2 *>(in + sg[uu]));
+                old[uu] = o.x;
+                oldx[uu] = o.y;
+              } else {
+                old[uu] = ldcg(in + sg[uu]);
+                oldx[uu] = 0u;
+              }
             }
           }
 #pragma unroll
           for (int uu = 0; uu < 4; ++uu) {
             const uint32_t q = q0 + uu * BT;
             if (q < nq) {
-              out[sg[uu]] = (old[uu] & ~cp[uu]) | (wv[uu] & cp[uu]);
+              const uint32_t nv = (old[uu] & ~cp[uu]) | (wv[uu] & cp[uu]);
               if (is_x)
-                out[xsig + sg[uu]] =
-                    (oldx[uu] & ~cp[uu] & ~cpx[uu]) | (wx[uu] & cp[uu] & ~cpx[uu]) | cpx[uu];
+                *reinterpret_cast<uint2 *>(out + sg[uu]) = make_uint2(
+                    nv, (oldx[uu] & ~cp[uu] & ~cpx[uu]) | (wx[uu] & cp[uu] & ~cpx[uu]) | cpx[uu]);
+              else
+                out[sg[uu]] = nv;
             }
           }
         }
@@ -534,7 +572,9 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
                           const uint32_t *in, uint32_t *out, uint32_t lp, uint32_t pid0,
                           bool &failed, uint32_t &next_ticket, bool &have_next) {
   const int t = threadIdx.x;
-  const size_t base0 = (size_t)(2 * lp) * P.sig_per_snap, base1 = base0 + P.sig_per_snap;
+  // the pair's words: quads (v0, x0, v1, x1) at 4 * (lp * V + s) with
+  // xhalf, else (v0, v1) at 2 * (lp * sig + s)
+  const size_t pair_base = P.xhalf ? ((size_t)lp * P.vsig) << 2 : ((size_t)lp * P.sig_per_snap) << 1;
   size_t off = 0;
   uint32_t pid = pid0;
   for (;;) {
@@ -554,7 +594,6 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     const uint32_t num_srams = sh.meta[4], sram_off = sh.meta[5], R = sh.meta[6];
     const uint32_t num_dup = sh.meta[7];
     const bool is_x = sh.meta[8] != 0;
-    const uint32_t xsig = sh.meta[9] * 32u;
     const uint32_t *ch0 = script + off + 256 + 512 * (size_t)R;
     const bool has_sram = (num_srams | num_dup) != 0;
     const uint32_t nchunks = ns + (has_sram ? 2 : 1);
@@ -573,11 +612,13 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         if (ek < GR_SKIP) {
           const uint32_t *bp = (ek >> 31) ? out : in;
           const size_t sg = ek & 0x7fffffffu;
-          v[k].x = ldcg(bp + base0 + sg);
-          v[k].z = ldcg(bp + base1 + sg);
-          if (is_x) {
-            v[k].y = ldcg(bp + xsig + base0 + sg);
-            v[k].w = ldcg(bp + xsig + base1 + sg);
+          if (P.xhalf) {
+            v[k] = __ldcg(reinterpret_cast<const uint4 *>(bp + pair_base + (sg << 2)));
+            if (!is_x) v[k].y = v[k].w = 0u;
+          } else {
+            const uint2 q = __ldcg(reinterpret_cast<const uint2 *>(bp + pair_base + (sg << 1)));
+            v[k].x = q.x;
+            v[k].z = q.y;
           }
         }
       }
@@ -795,10 +836,18 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
             const uint32_t q = q0 + uu * BT;
             if (q < nq) {
               const size_t sg = (size_t)io_off * 32 + q;
-              o[uu][0] = ldcg(in + base0 + sg);
-              o[uu][1] = ldcg(in + base1 + sg);
-              o[uu][2] = is_x ? ldcg(in + xsig + base0 + sg) : 0u;
-              o[uu][3] = is_x ? ldcg(in + xsig + base1 + sg) : 0u;
+              if (is_x) {  // quad layout
+                const uint4 w = __ldcg(reinterpret_cast<const uint4 *>(in + pair_base + (sg << 2)));
+                o[uu][0] = w.x;
+                o[uu][1] = w.z;
+                o[uu][2] = w.y;
+                o[uu][3] = w.w;
+              } else {
+                const size_t w = pair_base + (sg << (P.xhalf ? 2 : 1));
+                o[uu][0] = ldcg(in + w);
+                o[uu][1] = ldcg(in + w + (P.xhalf ? 2 : 1));
+                o[uu][2] = o[uu][3] = 0u;
+              }
             }
           }
 #pragma unroll
@@ -812,12 +861,18 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
               const uint4 me = WO[q];
               const size_t sg = (size_t)io_off * 32 + q;
               const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
-              out[base0 + sg] = (o[uu][0] & ~cp0) | ((me.x ^ dinv) & cp0);
-              out[base1 + sg] = (o[uu][1] & ~cp1) | ((me.z ^ dinv) & cp1);
+              const uint32_t n0 = (o[uu][0] & ~cp0) | ((me.x ^ dinv) & cp0);
+              const uint32_t n1 = (o[uu][1] & ~cp1) | ((me.z ^ dinv) & cp1);
               if (is_x) {
                 const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
-                out[xsig + base0 + sg] = (o[uu][2] & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0;
-                out[xsig + base1 + sg] = (o[uu][3] & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1;
+                *reinterpret_cast<uint4 *>(out + pair_base + (sg << 2)) =
+                    make_uint4(n0, (o[uu][2] & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0, n1,
+                               (o[uu][3] & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1);
+              } else if (P.xhalf) {  // values only; the X words keep theirs
+                out[pair_base + (sg << 2)] = n0;
+                out[pair_base + (sg << 2) + 2] = n1;
+              } else {
+                *reinterpret_cast<uint2 *>(out + pair_base + (sg << 1)) = make_uint2(n0, n1);
               }
             }
           }
@@ -865,19 +920,14 @@ __device__ void prefetch_item_l2(const BatchParams &P, unsigned ms, const uint32
   const uint32_t script_lines = (uint32_t)((left < WINDOW ? left : WINDOW) / 32);
   for (uint32_t l = i0; l < GR_LINES + script_lines; l += n)
     prefetch_l2(l < GR_LINES ? gr + 32 * l : script + 32 * (l - GR_LINES));
-  // commit rows of the first partition: [io_off*32, +num_ios*32) of each
-  // lane word of the item and of their X planes
+  // commit rows of the first partition: signals [io_off*32, +num_ios*32)
+  // of the item's lane pair, contiguous in the interleaved layout
   const uint32_t ns = script[0], num_ios = script[2], io_off = script[3];
   if (ns == 0) return;
-  const bool is_x = script[8] != 0;
-  const size_t xsig = (size_t)script[9] * 32;
-  const size_t b0 = (size_t)(NL * (blockIdx.x % per)) * P.sig_per_snap + (size_t)io_off * 32;
-  const uint32_t rows = NL * (is_x ? 2 : 1);
-  for (uint32_t l = i0; l < rows * num_ios; l += n) {
-    const uint32_t r = l / num_ios, k = l % num_ios;  // row (lane word, plane), 128-byte line
-    const size_t base = b0 + (size_t)(is_x ? r >> 1 : r) * P.sig_per_snap + (is_x && (r & 1) ? xsig : 0);
-    prefetch_l2(prev + base + 32 * (size_t)k);
-  }
+  const uint32_t lane0 = NL * (blockIdx.x % per);
+  const size_t w0 = phys(P, lane0 & ~1u, (size_t)io_off * 32);
+  const uint32_t lines = num_ios * (P.xhalf ? 4 : 2);  // 32 signals x 16 or 8 bytes
+  for (uint32_t l = i0; l < lines; l += n) prefetch_l2(prev + w0 + 32 * (size_t)l);
 }
 
 // NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
@@ -901,7 +951,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
-  const size_t snap = P.sig_per_snap * P.lanes;
+  const size_t snap = P.sig_per_snap * P.lanes;  // lane-major record snapshot
 
   for (size_t c = 0; c < P.num_cycles; ++c) {
     const uint32_t *in = (c & 1) ? P.state_b : P.state_a;
@@ -923,7 +973,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
             if (i >= s0 && i < s0 + n) dst = d0 + (i - s0);
           }
         }
-        out[l * P.sig_per_snap + dst] = src[q];
+        out[phys(P, (uint32_t)l, dst)] = src[q];
       }
     }
     for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
@@ -1005,12 +1055,12 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
     for (size_t q = (size_t)blockIdx.x * BT + t; q < (size_t)P.n_po * P.lanes;
          q += (size_t)gridDim.x * BT) {
       const uint32_t po = (uint32_t)(q / P.lanes), l = (uint32_t)(q % P.lanes);
-      P.wave[(c * P.n_po + po) * P.lanes + l] = ldcg(out + (size_t)l * P.sig_per_snap + P.po_sig[po]);
+      P.wave[(c * P.n_po + po) * P.lanes + l] = ldcg(out + phys(P, l, P.po_sig[po]));
     }
-    if (P.record) {
+    if (P.record) {  // lane-major [lane][signal]
       uint32_t *dst = P.record + (c + 1) * snap;
       for (size_t q = (size_t)blockIdx.x * BT + t; q < snap; q += (size_t)gridDim.x * BT)
-        dst[q] = ldcg(out + q);
+        dst[q] = ldcg(out + phys(P, (uint32_t)(q / P.sig_per_snap), q % P.sig_per_snap));
     }
     // the recording reads `out`; the next cycle writes into `in`: the next
     // major-stage barrier already orders them, no extra barrier needed.
@@ -1209,6 +1259,20 @@ __global__ void jq_batched_count_kernel(const size_t *blocks_start, const uint32
 
 using namespace jqk;
 
+// Lane-major [lane][signal] snapshot <-> the interleaved batched state.
+__global__ void jq_batched_pack_kernel(const uint32_t *lm, uint32_t *st, uint32_t lanes,
+                                       size_t sig, int xhalf, int unpack) {
+  const size_t n = (size_t)lanes * sig;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const size_t w = phys(xhalf, sig / 2, sig, (uint32_t)(q / sig), q % sig);
+    if (unpack)
+      st[q] = lm[w];  // st: lane-major output, lm: batched input
+    else
+      st[w] = lm[q];
+  }
+}
+
 // Re-arms one slot's barrier, ticket and status before a launch.  A kernel
 // (not a host copy) so the reset is captured in CUDA graphs with the launch.
 __global__ void jq_batched_reset_kernel(int slot) {
@@ -1278,6 +1342,31 @@ int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
 }
 
 size_t jq_batched_gr_words(size_t num_partitions) { return (num_partitions + 1) * 8192; }
+
+size_t jq_batched_state_words(uint32_t lanes, size_t signals) {
+  return (size_t)((lanes + 1) & ~1u) * signals;
+}
+
+static int pack_launch(const uint32_t *src, uint32_t *dst, uint32_t lanes, size_t signals,
+                       int32_t x_interleaved, int unpack, void *stream) {
+  if (!src || !dst || lanes == 0 || signals == 0 || (x_interleaved && (signals & 1)))
+    return JQ_ERR_INVALID_ARG;
+  const size_t n = (size_t)lanes * signals;
+  const unsigned grid = (unsigned)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+  jq_batched_pack_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(src, dst, lanes, signals,
+                                                                   x_interleaved != 0, unpack);
+  return cudaGetLastError() == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
+}
+
+int jq_batched_pack_state(const uint32_t *lane_major, uint32_t lanes, size_t signals,
+                          int32_t x_interleaved, uint32_t *state, void *stream) {
+  return pack_launch(lane_major, state, lanes, signals, x_interleaved, 0, stream);
+}
+
+int jq_batched_unpack_state(const uint32_t *state, uint32_t lanes, size_t signals,
+                            int32_t x_interleaved, uint32_t *lane_major, void *stream) {
+  return pack_launch(state, lane_major, lanes, signals, x_interleaved, 1, stream);
+}
 
 int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
                        size_t blocks_data_len, size_t num_blocks, size_t num_major_stages,
@@ -1351,6 +1440,9 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.sram_words = a->sram_words_per_stream;
   P.num_cycles = a->num_cycles;
   P.sig_per_snap = a->signals_per_snapshot;
+  if (a->x_interleaved && (P.sig_per_snap & 1)) return JQ_ERR_INVALID_ARG;
+  P.xhalf = a->x_interleaved != 0;
+  P.vsig = P.xhalf ? P.sig_per_snap / 2 : P.sig_per_snap;
   P.state_a = a->state_a;
   P.state_b = a->state_b;
   P.stim = a->stimulus;

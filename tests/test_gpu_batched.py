@@ -101,7 +101,7 @@ def test_multi_design_single_launch_matches_separate_runs():
         finals.append(B.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, -1))
     C = batched.CombinedScript(scripts)
     BC = batched.BatchedSim(C, lanes)
-    snap0 = np.concatenate([bt[0] for bt in bts], axis=-1)
+    snap0 = C.combine_states([bt[0] for bt in bts])
     assert snap0.shape == (lanes, BC.sig)
     BC.load_state(snap0)
     BC.reset_sram()
@@ -117,6 +117,4 @@ def test_multi_design_single_launch_matches_separate_runs():
     assert BC.status() == 0
     got = BC.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, -1)
     for d, s in enumerate(scripts):
-        lo = C.state_base[d] * 32
-        n = 2 * s.reg_io_state_size * 32
-        assert np.array_equal(got[:, lo:lo + n], finals[d]), f"design {d}"
+        assert np.array_equal(C.design_state(d, got), finals[d]), f"design {d}"
