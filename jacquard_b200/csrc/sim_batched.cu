@@ -1092,9 +1092,11 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 // Bits 16+i of the second flag word mark owned position i as read from
 // outside its stage; only those are stored.  In deep stages threads t < 8
 // hold the warp-0 flags there instead and store all their positions.
-// Unneeded global-read positions get source 0xfffffffe (neither loaded nor
-// stored).  Dead positions are neither stored nor read, so the state they
-// leave in shared memory is never observed.
+// The global-read positions stage 0 needs are compacted into slots 0, 1, ...
+// of the partition's source row (the rest GR_SKIP: neither loaded nor
+// stored), and stage 0's sources name slots.  Dead positions are neither
+// stored nor read, so the state they leave in shared memory is never
+// observed.
 
 __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     const size_t *blocks_start, const uint32_t *src, uint32_t *dst, unsigned entries,
@@ -1102,6 +1104,8 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
   __shared__ uint32_t need_bits[256];  // previous tree's positions read by needed gathers
   __shared__ uint32_t ext_bits[256];   // this stage's positions read from outside
   __shared__ uint8_t live[8192];
+  __shared__ uint16_t slot_of[8192];   // global-read position -> compacted slot
+  __shared__ uint32_t warp_sum[BT / 32];
   const unsigned e = blockIdx.x;
   if (e >= entries) return;
   const uint32_t t = threadIdx.x;
@@ -1114,6 +1118,36 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     const uint32_t is_last = src[off + 1], nio = src[off + 2], R = src[off + 6];
     const uint32_t *ch = src + off + 256 + 512 * (size_t)R;
     uint32_t *dch = dst + off + 256 + 512 * (size_t)R;
+    int deep0 = 0, flat0 = 0;
+    // Source entries of one boomerang chunk C -> D: plane m>>2, word m&3
+    // holds entries 8*(m>>2) + 2*(m&3) + {0, 1}; entry k < 8 is input a of
+    // position 4096+u+512k (source q = u+512k), entry 8+k its input b
+    // (q + 4096).  Marks the needed sources in need_bits; with `write` the
+    // words are stored, with `slots` a source names its compacted
+    // global-read slot instead of its position.
+    auto write_entries = [&](const uint32_t *C, uint32_t *D, int deep, int flat, bool write,
+                             bool slots) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t en = 8 * (m >> 2) + 2 * (m & 3) + h;
+          const uint32_t q = (en < 8) ? u + 512 * en : u + 512 * (en - 8) + 4096;
+          const uint32_t P = 4096 + (q & 4095u);
+          const bool ob = (C[4096 + 4 * (P >> 5) + 2] >> (P & 31)) & 1u;
+          const uint32_t sp = perm_src(C, q) & 8191u;
+          const bool need = live[P] && !(en >= 8 && ob);
+          if (need && !slots) atomicOr(&need_bits[sp >> 5], 1u << (sp & 31));
+          const uint32_t a = slots ? (need ? slot_of[sp] : 0u) : sp;
+          const uint32_t entry = sw(a) | ((uint32_t)need << 15) |
+                                 ((en == 0 && !deep) ? (1u << 13) : 0u) |
+                                 ((en == 1 && flat) ? (1u << 13) : 0u);
+          w |= entry << (16 * h);
+        }
+        if (write) D[4 * ((m >> 2) * BT + t) + (m & 3)] = w;
+      }
+    };
     for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;  // nothing reads the last stage
     __syncthreads();
     for (int ci = (int)ns - 1; ci >= 0; --ci) {
@@ -1144,30 +1178,13 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
       int upper = 0;  // any live position in [512, 4096) (levels 2..4)
       for (uint32_t c = 512 + t; c < 4096; c += BT) upper |= live[c];
       const int flat = !deep && !__syncthreads_or(upper);  // level 1 only
+      deep0 = deep;
+      flat0 = flat;
       for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;
       __syncthreads();
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        // plane m>>2, word m&3: entries 8*(m>>2) + 2*(m&3) + {0, 1}; entry
-        // k < 8 is input a of position 4096+u+512k (source q = u+512k),
-        // entry 8+k its input b (q + 4096)
-        uint32_t w = 0;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const uint32_t en = 8 * (m >> 2) + 2 * (m & 3) + h;
-          const uint32_t q = (en < 8) ? u + 512 * en : u + 512 * (en - 8) + 4096;
-          const uint32_t P = 4096 + (q & 4095u);
-          const bool ob = (C[4096 + 4 * (P >> 5) + 2] >> (P & 31)) & 1u;
-          const uint32_t sp = perm_src(C, q) & 8191u;
-          const bool need = live[P] && !(en >= 8 && ob);
-          if (need) atomicOr(&need_bits[sp >> 5], 1u << (sp & 31));
-          const uint32_t entry = sw(sp) | ((uint32_t)need << 15) |
-                                 ((en == 0 && !deep) ? (1u << 13) : 0u) |
-                                 ((en == 1 && flat) ? (1u << 13) : 0u);
-          w |= entry << (16 * h);
-        }
-        D[4 * ((m >> 2) * BT + t) + (m & 3)] = w;
-      }
+      // stage 0's entries name global-read slots, known once the needed
+      // global-read positions are compacted (below)
+      write_entries(C, D, deep, flat, ci > 0, false);
       uint32_t A = 0, B = 0;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
@@ -1202,9 +1219,10 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     // bit ends up most significant, i.e. at position 32t + total - 1
     // (csrc/kernel_v1_impl.cuh:87-154).  Positions no needed stage-0 gather
     // reads are marked GR_SKIP, unfilled needed ones GR_EMPTY.
+    uint32_t *row = gr_sources + pid * 8192;
     if (t < 256) {
       const uint32_t *gr = src + off + 256;
-      uint32_t *G = gr_sources + pid * 8192 + 32 * t;
+      uint32_t *G = row + 32 * t;
       uint32_t total = 0;
       for (uint32_t r = 0; r < R; ++r) total += __popc(gr[512 * r + 2 * t + 1]);
       if (total > 32) total = 32;  // at most 32 bits per thread (script validator)
@@ -1221,10 +1239,42 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         }
       }
       for (uint32_t k = total; k < 32; ++k) G[k] = GR_EMPTY;
-      const uint32_t nb = need_bits[t];  // positions 32t .. 32t+31
-      for (uint32_t k = 0; k < 32; ++k)
-        if (!((nb >> k) & 1u)) G[k] = GR_SKIP;
     }
+    __syncthreads();
+    // Compaction: the needed positions, in position order, take slots 0, 1,
+    // ... of the row (the rest GR_SKIP), so the kernel's global read has no
+    // idle lanes; stage 0 gathers from the slots.  Thread t owns positions
+    // 16t .. 16t+15.
+    {
+      const uint32_t keep = (need_bits[t >> 1] >> (16 * (t & 1))) & 0xffffu;
+      uint32_t vals[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) vals[j] = (keep >> j) & 1u ? row[16 * t + j] : 0u;
+      const uint32_t cnt = __popc(keep);
+      uint32_t incl = cnt;  // block-wide exclusive scan of cnt
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+        if ((t & 31) >= (uint32_t)d) incl += o;
+      }
+      if ((t & 31) == 31) warp_sum[t >> 5] = incl;
+      __syncthreads();  // every row read done, warp sums visible
+      uint32_t base = incl - cnt;
+      for (uint32_t w = 0; w < (t >> 5); ++w) base += warp_sum[w];
+      uint32_t n = 0;
+      for (uint32_t w = 0; w < BT / 32; ++w) n += warp_sum[w];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if ((keep >> j) & 1u) {
+          row[base] = vals[j];
+          slot_of[16 * t + j] = (uint16_t)base;
+          ++base;
+        }
+      }
+      for (uint32_t i = n + t; i < 8192; i += BT) row[i] = GR_SKIP;
+    }
+    __syncthreads();
+    write_entries(ch, dch, deep0, flat0, true, true);
     for (uint32_t ci = ns; ci < ns + 2; ++ci) {
       const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
       uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
