@@ -272,6 +272,10 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
       const uint32_t hw = sh.meta[128 + slot / 2];
       my_hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
     }
+    // compact form (jq_batched_prepare): stages as dense slot lists, hooks
+    // naming 32-slot blocks of the stage's region
+    const bool compact = sh.meta[10] & 1u;
+    uint32_t prev_base = 0;
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
       const uint32_t b = ci & 1;
       uint32_t *C = chunks + b * STAGE_WORDS;
@@ -296,7 +300,55 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     if (t == 0) mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.timeout); \
     return;                                                            \
   }
-      if (ci < ns) {
+      // hooks of a compact stage: 32-slot blocks of its region
+#define JQ_HOOKS_COMPACT(stage, pbase)                                                        \
+  for (uint32_t hm = __ballot_sync(0xffffffffu, (my_hook >> 8) == (stage)); hm; hm &= hm - 1) { \
+    const uint32_t j = __ffs(hm) - 1;                                                         \
+    const uint32_t blk = __shfl_sync(0xffffffffu, my_hook, j) & 255u;                         \
+    WO[(warp_i + 16 * j) * 32 + lane_i] = Sb0[(pbase) + 32 * blk + lane_i];                   \
+  }
+      if (compact && ci == ns && ok) JQ_HOOKS_COMPACT(ns - 1, prev_base)
+      if (ci < ns && compact) {
+        // ---------------- compact stage ci: one word per live position; it
+        // reads the previous region and writes its own, disjoint one, so one
+        // barrier per stage (a stage-0 region that overlaps the global read
+        // is computed in full before it is stored)
+        const uint32_t n = ok ? C[4096] : 0u, base = ok ? C[4097] : 0u;
+#define JQ_COMPACT_EVAL(i, r)                                                              \
+  {                                                                                        \
+    const uint32_t en = C[i];                                                              \
+    const uint2 ga = ((en >> 29) & 1u) ? make_uint2(0, 0) : Sb0[en & 8191u];               \
+    const uint2 gb = ((en >> 30) & 1u) ? make_uint2(0, 0) : Sb0[(en >> 13) & 8191u];       \
+    xand(ga.x, ga.y, gb.x, gb.y, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u),           \
+         0u - ((en >> 28) & 1u), r.x, r.y);                                                \
+  }
+        // slots below ov (stage 0 only) lie over the global read: held in
+        // registers until every thread has gathered
+        const uint32_t ov = ok ? C[4098] : 0u;
+        uint2 h0 = make_uint2(0, 0), h1 = h0;
+        if (ok) {
+          if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
+#pragma unroll 2
+          for (uint32_t i = t; i < n; i += BT) {
+            uint2 r;
+            JQ_COMPACT_EVAL(i, r)
+            if (i >= ov)
+              Sb0[base + i] = r;
+            else if (i < BT)
+              h0 = r;
+            else
+              h1 = r;
+          }
+        }
+        JQ_FAIL_IF(!ok)
+        if (ov) {
+          if (t < ov) Sb0[base + t] = h0;
+          if (t + BT < ov) Sb0[base + t + BT] = h1;
+          __syncthreads();
+        }
+#undef JQ_COMPACT_EVAL
+        prev_base = base;
+      } else if (ci < ns) {
         // ---------------- boomerang stage ci
         const uint2 *Sp = (ci & 1) ? Sb1 : Sb0;
         uint2 *Sn = (ci & 1) ? Sb0 : Sb1;
@@ -544,6 +596,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
   }
 }
 #undef JQ_FAIL_IF
+#undef JQ_HOOKS_COMPACT
 
 // X-propagating AND of two lane words at once: (v0, x0, v1, x1) operands.
 __device__ __forceinline__ uint4 xand2(uint4 a, uint4 b, uint32_t xa, uint32_t xb, uint32_t ob) {
@@ -637,6 +690,10 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       const uint32_t hw = sh.meta[128 + slot / 2];
       my_hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
     }
+    // compact form (jq_batched_prepare): stages as dense slot lists, hooks
+    // naming 32-slot blocks of the stage's region
+    const bool compact = sh.meta[10] & 1u;
+    uint32_t prev_base = 0;
     for (uint32_t ci = 0; ci < nchunks; ++ci) {
       const uint32_t b = ci & 1;
       uint32_t *C = chunks + b * STAGE_WORDS;
@@ -656,7 +713,48 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     if (t == 0) mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.timeout); \
     return;                                                            \
   }
-      if (ci < ns) {
+#define JQ_HOOKS_COMPACT(stage, pbase)                                                        \
+  for (uint32_t hm = __ballot_sync(0xffffffffu, (my_hook >> 8) == (stage)); hm; hm &= hm - 1) { \
+    const uint32_t j = __ffs(hm) - 1;                                                         \
+    const uint32_t blk = __shfl_sync(0xffffffffu, my_hook, j) & 255u;                         \
+    WO[(warp_i + 16 * j) * 32 + lane_i] = S[(pbase) + 32 * blk + lane_i];                     \
+  }
+      if (compact && ci == ns && ok) JQ_HOOKS_COMPACT(ns - 1, prev_base)
+      if (ci < ns && compact) {
+        // ---------------- compact stage ci (see run_item)
+        const uint32_t n = ok ? C[4096] : 0u, base = ok ? C[4097] : 0u;
+#define JQ_COMPACT_EVAL(i, r)                                                                \
+  {                                                                                          \
+    const uint32_t en = C[i];                                                                \
+    const uint4 ga = ((en >> 29) & 1u) ? make_uint4(0, 0, 0, 0) : S[en & 8191u];             \
+    const uint4 gb = ((en >> 30) & 1u) ? make_uint4(0, 0, 0, 0) : S[(en >> 13) & 8191u];     \
+    r = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u), 0u - ((en >> 28) & 1u)); \
+  }
+        const uint32_t ov = ok ? C[4098] : 0u;  // held slots (stage 0)
+        uint4 h0 = make_uint4(0, 0, 0, 0), h1 = h0;
+        if (ok) {
+          if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
+#pragma unroll 2
+          for (uint32_t i = t; i < n; i += BT) {
+            uint4 r;
+            JQ_COMPACT_EVAL(i, r)
+            if (i >= ov)
+              S[base + i] = r;
+            else if (i < BT)
+              h0 = r;
+            else
+              h1 = r;
+          }
+        }
+        JQ_FAIL_IF(!ok)
+        if (ov) {
+          if (t < ov) S[base + t] = h0;
+          if (t + BT < ov) S[base + t + BT] = h1;
+          __syncthreads();
+        }
+#undef JQ_COMPACT_EVAL
+        prev_base = base;
+      } else if (ci < ns) {
         // ---------------- boomerang stage ci
         uint4 v1[8];
         uint32_t A = 0, B = 0, sm = 0;
@@ -889,6 +987,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
   }
 }
 #undef JQ_FAIL_IF
+#undef JQ_HOOKS_COMPACT
 
 __device__ __forceinline__ void prefetch_l2(const void *p) {
   asm volatile("prefetch.L2 [%0];" ::"l"(p));
@@ -1098,14 +1197,52 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
 // stored nor read, so the state they leave in shared memory is never
 // observed.
 
+constexpr uint32_t COMPACT_MAX_STAGES = 32;
+
+// Shared memory of the prepare kernel (dynamic).
+struct PrepShared {
+  uint32_t need_bits[256];  // previous tree's positions read by needed gathers
+  uint32_t ext_bits[256];   // this stage's positions read from outside
+  uint32_t ext_all[COMPACT_MAX_STAGES][256];  // ext_bits of every stage
+  uint32_t warp_sum[BT / 32];
+  uint32_t hmask[8];        // hooked 32-position groups of a stage
+  uint16_t blk_of[256];     // hooked group -> 32-slot block of its region
+  uint16_t slot_prev[8192];  // previous stage's position -> shared-memory word
+  uint16_t slot_cur[8192];
+  uint16_t pos_of[4096];    // region slot -> position
+  uint8_t live[8192];
+};
+
+// Exclusive prefix sum of v over the CTA; *total receives the sum.  Every
+// thread calls it.
+__device__ uint32_t block_excl_scan(uint32_t v, uint32_t *warp_sum, uint32_t *total) {
+  const uint32_t t = threadIdx.x;
+  uint32_t incl = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+    if ((t & 31) >= (uint32_t)d) incl += o;
+  }
+  __syncthreads();  // earlier readers of warp_sum are done
+  if ((t & 31) == 31) warp_sum[t >> 5] = incl;
+  __syncthreads();
+  uint32_t base = incl - v, n = 0;
+  for (uint32_t w = 0; w < BT / 32; ++w) {
+    if (w < (t >> 5)) base += warp_sum[w];
+    n += warp_sum[w];
+  }
+  *total = n;
+  return base;
+}
+
 __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     const size_t *blocks_start, const uint32_t *src, uint32_t *dst, unsigned entries,
     const uint32_t *part_base, uint32_t *gr_sources, size_t num_partitions) {
-  __shared__ uint32_t need_bits[256];  // previous tree's positions read by needed gathers
-  __shared__ uint32_t ext_bits[256];   // this stage's positions read from outside
-  __shared__ uint8_t live[8192];
-  __shared__ uint16_t slot_of[8192];   // global-read position -> compacted slot
-  __shared__ uint32_t warp_sum[BT / 32];
+  extern __shared__ __align__(16) uint8_t prep_dyn[];
+  PrepShared &ps = *reinterpret_cast<PrepShared *>(prep_dyn);
+  uint32_t *const need_bits = ps.need_bits;
+  uint32_t *const ext_bits = ps.ext_bits;
+  uint8_t *const live = ps.live;
   const unsigned e = blockIdx.x;
   if (e >= entries) return;
   const uint32_t t = threadIdx.x;
@@ -1118,13 +1255,13 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     const uint32_t is_last = src[off + 1], nio = src[off + 2], R = src[off + 6];
     const uint32_t *ch = src + off + 256 + 512 * (size_t)R;
     uint32_t *dch = dst + off + 256 + 512 * (size_t)R;
-    int deep0 = 0, flat0 = 0;
+    int deep0 = 0, flat0 = 0, all_flat = 1;
     // Source entries of one boomerang chunk C -> D: plane m>>2, word m&3
     // holds entries 8*(m>>2) + 2*(m&3) + {0, 1}; entry k < 8 is input a of
     // position 4096+u+512k (source q = u+512k), entry 8+k its input b
     // (q + 4096).  Marks the needed sources in need_bits; with `write` the
-    // words are stored, with `slots` a source names its compacted
-    // global-read slot instead of its position.
+    // words are stored, with `slots` a source names the shared-memory word
+    // of its compacted global-read slot instead of its position.
     auto write_entries = [&](const uint32_t *C, uint32_t *D, int deep, int flat, bool write,
                              bool slots) {
 #pragma unroll
@@ -1139,8 +1276,8 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
           const uint32_t sp = perm_src(C, q) & 8191u;
           const bool need = live[P] && !(en >= 8 && ob);
           if (need && !slots) atomicOr(&need_bits[sp >> 5], 1u << (sp & 31));
-          const uint32_t a = slots ? (need ? slot_of[sp] : 0u) : sp;
-          const uint32_t entry = sw(a) | ((uint32_t)need << 15) |
+          const uint32_t a = slots ? (need ? ps.slot_prev[sp] : 0u) : sw(sp);
+          const uint32_t entry = a | ((uint32_t)need << 15) |
                                  ((en == 0 && !deep) ? (1u << 13) : 0u) |
                                  ((en == 1 && flat) ? (1u << 13) : 0u);
           w |= entry << (16 * h);
@@ -1150,6 +1287,7 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     };
     for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;  // nothing reads the last stage
     __syncthreads();
+    // ---- pass 1, last stage to first: liveness and the tree-form chunks
     for (int ci = (int)ns - 1; ci >= 0; --ci) {
       const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
       uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
@@ -1180,6 +1318,9 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
       const int flat = !deep && !__syncthreads_or(upper);  // level 1 only
       deep0 = deep;
       flat0 = flat;
+      all_flat &= flat;
+      if (ci < (int)COMPACT_MAX_STAGES)
+        for (uint32_t w = t; w < 256; w += BT) ps.ext_all[ci][w] = ext_bits[w];
       for (uint32_t w = t; w < 256; w += BT) need_bits[w] = 0;
       __syncthreads();
       // stage 0's entries name global-read slots, known once the needed
@@ -1217,8 +1358,7 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     // global-read sources: thread t < 256 appends its masked bits round by
     // round, walking each mask from the lowest set bit; the first appended
     // bit ends up most significant, i.e. at position 32t + total - 1
-    // (csrc/kernel_v1_impl.cuh:87-154).  Positions no needed stage-0 gather
-    // reads are marked GR_SKIP, unfilled needed ones GR_EMPTY.
+    // (csrc/kernel_v1_impl.cuh:87-154); unfilled positions are GR_EMPTY.
     uint32_t *row = gr_sources + pid * 8192;
     if (t < 256) {
       const uint32_t *gr = src + off + 256;
@@ -1241,47 +1381,138 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
       for (uint32_t k = total; k < 32; ++k) G[k] = GR_EMPTY;
     }
     __syncthreads();
-    // Compaction: the needed positions, in position order, take slots 0, 1,
-    // ... of the row (the rest GR_SKIP), so the kernel's global read has no
-    // idle lanes; stage 0 gathers from the slots.  Thread t owns positions
-    // 16t .. 16t+15.
+    // Compaction: the global-read positions stage 0 needs, in position
+    // order, take slots 0, 1, ... of the row (the rest GR_SKIP), so the
+    // kernel's global read has no idle lanes; slot s lands in shared-memory
+    // word sw(s).  Thread t owns positions 16t .. 16t+15.
+    uint32_t n_gr = 0;
     {
       const uint32_t keep = (need_bits[t >> 1] >> (16 * (t & 1))) & 0xffffu;
       uint32_t vals[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) vals[j] = (keep >> j) & 1u ? row[16 * t + j] : 0u;
-      const uint32_t cnt = __popc(keep);
-      uint32_t incl = cnt;  // block-wide exclusive scan of cnt
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
-        if ((t & 31) >= (uint32_t)d) incl += o;
-      }
-      if ((t & 31) == 31) warp_sum[t >> 5] = incl;
-      __syncthreads();  // every row read done, warp sums visible
-      uint32_t base = incl - cnt;
-      for (uint32_t w = 0; w < (t >> 5); ++w) base += warp_sum[w];
-      uint32_t n = 0;
-      for (uint32_t w = 0; w < BT / 32; ++w) n += warp_sum[w];
+      uint32_t base = block_excl_scan(__popc(keep), ps.warp_sum, &n_gr);  // row reads done
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        if ((keep >> j) & 1u) {
-          row[base] = vals[j];
-          slot_of[16 * t + j] = (uint16_t)base;
-          ++base;
-        }
+        ps.slot_prev[16 * t + j] = (keep >> j) & 1u ? (uint16_t)sw(base) : (uint16_t)0xffffu;
+        if ((keep >> j) & 1u) row[base++] = vals[j];
       }
-      for (uint32_t i = n + t; i < 8192; i += BT) row[i] = GR_SKIP;
+      for (uint32_t i = n_gr + t; i < 8192; i += BT) row[i] = GR_SKIP;
     }
     __syncthreads();
     write_entries(ch, dch, deep0, flat0, true, true);
+    // ---- compact form, when every stage evaluates only level 1 and only
+    // positions read from outside.  Stage ci's live positions get the slots
+    // of a region of shared memory (its hooked 32-position groups as 32-slot
+    // blocks, then the other positions), at the top of the tree buffer for
+    // even ci and at the bottom for odd ci, so a stage never writes what it
+    // reads and needs one barrier; the global read (slot s at word sw(s),
+    // below 32 * ceil(n_gr / 32)) sits at the bottom.  Where stage 0's region
+    // reaches into it, the first `ov` slots of stage 0 (at most 2 per
+    // thread) are held until every thread has read the global read.  The
+    // chunk becomes one word per slot: source words a | b << 13, flags xa <<
+    // 26, xb << 27, ob << 28, zero-source flags << 29 (a) and << 30 (b);
+    // words 4096, 4097, 4098 hold the slot count, the region's first word
+    // and ov.  Hooks are rewritten to (stage << 8) | block.  Metadata word 10
+    // bit 0 marks the form.
+    bool compact = all_flat && ns <= COMPACT_MAX_STAGES;
+    if (compact) {
+      for (uint32_t ci = 0; ci < ns; ++ci) {
+        const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
+        uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
+        const uint32_t *ex = ps.ext_all[ci];
+        if (t < 8) ps.hmask[t] = 0;
+        __syncthreads();
+        for (uint32_t slot = t; slot < nio; slot += BT) {
+          const uint32_t hw = src[off + 128 + slot / 2];
+          const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+          if ((hook >> 8) == ci) atomicOr(&ps.hmask[(hook & 255u) >> 5], 1u << (hook & 31u));
+        }
+        __syncthreads();
+        const bool hooked_t = t < 256 && ((ps.hmask[t >> 5] >> (t & 31)) & 1u);
+        uint32_t nh = 0;
+        const uint32_t bg = block_excl_scan(hooked_t ? 1u : 0u, ps.warp_sum, &nh);
+        if (hooked_t) ps.blk_of[t] = (uint16_t)bg;
+        // other level-1 positions read from outside: thread t owns 4096+8t..+7
+        uint32_t mine = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const uint32_t pp = 4096 + 8 * t + j;
+          const bool hk = (ps.hmask[pp >> 10] >> ((pp >> 5) & 31)) & 1u;
+          if (((ex[pp >> 5] >> (pp & 31)) & 1u) && !hk) mine |= 1u << j;
+        }
+        uint32_t no = 0;
+        uint32_t rk = block_excl_scan(__popc(mine), ps.warp_sum, &no);
+        const uint32_t n = 32 * nh + no;
+        const uint32_t base = (ci & 1) ? 0u : 8192u - n;
+        const uint32_t gr_top = (n_gr + 31) & ~31u;
+        const uint32_t ov = (ci == 0 && gr_top > base) ? gr_top - base : 0u;
+        if (ov > 2 * BT) {  // stage 0 only (uniform): keep the tree form
+          compact = false;
+          break;
+        }
+        for (uint32_t pp = t; pp < 8192; pp += BT) ps.slot_cur[pp] = 0xffffu;
+        __syncthreads();
+        for (uint32_t pp = t; pp < 8192; pp += BT) {
+          const uint32_t g = pp >> 5;
+          if ((ps.hmask[g >> 5] >> (g & 31)) & 1u) {
+            const uint32_t sl = 32 * ps.blk_of[g] + (pp & 31);
+            ps.slot_cur[pp] = (uint16_t)(base + sl);
+            ps.pos_of[sl] = (uint16_t)pp;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if ((mine >> j) & 1u) {
+            const uint32_t pp = 4096 + 8 * t + j, sl = 32 * nh + rk++;
+            ps.slot_cur[pp] = (uint16_t)(base + sl);
+            ps.pos_of[sl] = (uint16_t)pp;
+          }
+        }
+        __syncthreads();
+        for (uint32_t i = t; i < n; i += BT) {
+          const uint32_t P = ps.pos_of[i];
+          const uint32_t *F = C + 4096 + 4 * (P >> 5);
+          const uint32_t xa = (F[0] >> (P & 31)) & 1u, xb = (F[1] >> (P & 31)) & 1u,
+                         ob = (F[2] >> (P & 31)) & 1u;
+          const uint32_t sa = perm_src(C, P - 4096) & 8191u, sb = perm_src(C, P) & 8191u;
+          // a source of stage >= 1 at position 0 is the constant 0
+          const uint32_t wa = (ci > 0 && sa == 0) ? 0xffffu : ps.slot_prev[sa];
+          const uint32_t wb = (ob || (ci > 0 && sb == 0)) ? 0xffffu : ps.slot_prev[sb];
+          const uint32_t za = wa == 0xffffu, zb = wb == 0xffffu;
+          D[i] = (za ? 0u : wa) | ((zb ? 0u : wb) << 13) | (xa << 26) | (xb << 27) | (ob << 28) |
+                 (za << 29) | (zb << 30);
+        }
+        if (t == 0) {
+          D[4096] = n;
+          D[4097] = base;
+          D[4098] = ov;
+        }
+        if (t < 128 && 2 * t < nio) {  // meta word 128 + t: hooks of slots 2t, 2t+1
+          uint32_t w = dst[off + 128 + t];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t hk = (w >> (16 * h)) & 0xffffu;
+            if (2 * t + h < nio && (hk >> 8) == ci) {
+              const uint32_t nw = (ci << 8) | ps.blk_of[hk & 255u];
+              w = (w & ~(0xffffu << (16 * h))) | (nw << (16 * h));
+            }
+          }
+          dst[off + 128 + t] = w;
+        }
+        __syncthreads();
+        for (uint32_t pp = t; pp < 8192; pp += BT) ps.slot_prev[pp] = ps.slot_cur[pp];
+        __syncthreads();
+      }
+    }
+    if (t == 0) dst[off + 10] = compact ? 1u : 0u;
     for (uint32_t ci = ns; ci < ns + 2; ++ci) {
       const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
       uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
       for (uint32_t q2 = t; q2 < 4096; q2 += BT)
         D[q2] = perm_src(C, 2 * q2) | (perm_src(C, 2 * q2 + 1) << 16);
     }
-    __syncthreads();  // need_bits read before the next partition clears it
+    __syncthreads();  // shared state read before the next partition reuses it
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
     ++pid;
     if (is_last) break;
@@ -1454,10 +1685,17 @@ int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
                              cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
     rc = JQ_ERR_CUDA;
   } else {
-    jq_batched_prepare_kernel<<<(unsigned)entries, BT, 0, st>>>(
-        blocks_start, blocks_data, out, (unsigned)entries, part_base, gr_sources, num_partitions);
-    if (cudaGetLastError() != cudaSuccess) rc = JQ_ERR_LAUNCH;
-    else if (cudaStreamSynchronize(st) != cudaSuccess) rc = JQ_ERR_CUDA;
+    const int psmem = (int)sizeof(PrepShared);
+    if (cudaFuncSetAttribute(jq_batched_prepare_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, psmem) != cudaSuccess) {
+      rc = JQ_ERR_LAUNCH;
+    } else {
+      jq_batched_prepare_kernel<<<(unsigned)entries, BT, psmem, st>>>(
+          blocks_start, blocks_data, out, (unsigned)entries, part_base, gr_sources,
+          num_partitions);
+      if (cudaGetLastError() != cudaSuccess) rc = JQ_ERR_LAUNCH;
+      else if (cudaStreamSynchronize(st) != cudaSuccess) rc = JQ_ERR_CUDA;
+    }
   }
   free(h);
   return rc;
