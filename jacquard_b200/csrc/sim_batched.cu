@@ -322,28 +322,30 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
     xand(ga.x, ga.y, gb.x, gb.y, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u),           \
          0u - ((en >> 28) & 1u), r.x, r.y);                                                \
   }
-        // slots below ov (stage 0 only) lie over the global read: held in
-        // registers until every thread has gathered
+        // slots below ov (stage 0 only, at most 4 * BT) lie over the global
+        // read: held in registers until every thread has gathered
         const uint32_t ov = ok ? C[4098] : 0u;
-        uint2 h0 = make_uint2(0, 0), h1 = h0;
+        uint2 h[4] = {make_uint2(0, 0), make_uint2(0, 0), make_uint2(0, 0), make_uint2(0, 0)};
         if (ok) {
           if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
-#pragma unroll 2
-          for (uint32_t i = t; i < n; i += BT) {
+          // n <= 4096 slots: at most 8 per thread
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const uint32_t i = t + BT * k;
+            if (i >= n) break;
             uint2 r;
             JQ_COMPACT_EVAL(i, r)
-            if (i >= ov)
-              Sb0[base + i] = r;
-            else if (i < BT)
-              h0 = r;
+            if (k < 4 && i < ov)
+              h[k < 4 ? k : 0] = r;
             else
-              h1 = r;
+              Sb0[base + i] = r;
           }
         }
         JQ_FAIL_IF(!ok)
         if (ov) {
-          if (t < ov) Sb0[base + t] = h0;
-          if (t + BT < ov) Sb0[base + t + BT] = h1;
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (t + BT * k < ov) Sb0[base + t + BT * k] = h[k];
           __syncthreads();
         }
 #undef JQ_COMPACT_EVAL
@@ -731,25 +733,27 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     r = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u), 0u - ((en >> 28) & 1u)); \
   }
         const uint32_t ov = ok ? C[4098] : 0u;  // held slots (stage 0)
-        uint4 h0 = make_uint4(0, 0, 0, 0), h1 = h0;
+        uint4 h[4] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
         if (ok) {
           if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
-#pragma unroll 2
-          for (uint32_t i = t; i < n; i += BT) {
+          // n <= 4096 slots: at most 8 per thread
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const uint32_t i = t + BT * k;
+            if (i >= n) break;
             uint4 r;
             JQ_COMPACT_EVAL(i, r)
-            if (i >= ov)
-              S[base + i] = r;
-            else if (i < BT)
-              h0 = r;
+            if (k < 4 && i < ov)
+              h[k < 4 ? k : 0] = r;
             else
-              h1 = r;
+              S[base + i] = r;
           }
         }
         JQ_FAIL_IF(!ok)
         if (ov) {
-          if (t < ov) S[base + t] = h0;
-          if (t + BT < ov) S[base + t + BT] = h1;
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (t + BT * k < ov) S[base + t + BT * k] = h[k];
           __syncthreads();
         }
 #undef JQ_COMPACT_EVAL
@@ -1408,7 +1412,7 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     // even ci and at the bottom for odd ci, so a stage never writes what it
     // reads and needs one barrier; the global read (slot s at word sw(s),
     // below 32 * ceil(n_gr / 32)) sits at the bottom.  Where stage 0's region
-    // reaches into it, the first `ov` slots of stage 0 (at most 2 per
+    // reaches into it, the first `ov` slots of stage 0 (at most 4 per
     // thread) are held until every thread has read the global read.  The
     // chunk becomes one word per slot: source words a | b << 13, flags xa <<
     // 26, xb << 27, ob << 28, zero-source flags << 29 (a) and << 30 (b);
@@ -1447,7 +1451,7 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         const uint32_t base = (ci & 1) ? 0u : 8192u - n;
         const uint32_t gr_top = (n_gr + 31) & ~31u;
         const uint32_t ov = (ci == 0 && gr_top > base) ? gr_top - base : 0u;
-        if (ov > 2 * BT) {  // stage 0 only (uniform): keep the tree form
+        if (ov > 4 * BT) {  // stage 0 only (uniform): keep the tree form
           compact = false;
           break;
         }
