@@ -156,12 +156,24 @@ __device__ __forceinline__ size_t phys(const BatchParams &P, uint32_t l, size_t 
   return phys(P.xhalf, P.vsig, P.sig_per_snap, l, s);
 }
 
+constexpr uint32_t MAX_MAJOR_STAGES = 32;  // jq_simulate_batched's limit
+
 struct Shared {
   uint32_t meta[256];
   uint64_t bar[2];
   int ok;
   uint32_t ticket;
   int dyn;  // items of this major stage come from the ticket counter
+  // per major stage, resolved once per launch: its item count and, when it
+  // assigns items statically (at most one per CTA), this CTA's item: script
+  // offset (~0 when it has none), first partition, first partition's
+  // writeout count and IO offset
+  uint32_t st_items[MAX_MAJOR_STAGES];
+  size_t st_off[MAX_MAJOR_STAGES];
+  uint32_t st_pid[MAX_MAJOR_STAGES];
+  uint32_t st_nio[MAX_MAJOR_STAGES];
+  uint32_t st_io[MAX_MAJOR_STAGES];
+  size_t script_words;  // blocks_start[num_major_stages * num_blocks]
 };
 
 // One (block, lane) work item: the block's partition list for one lane word.
@@ -1004,33 +1016,39 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
 // rows `prev` its commit reads (a partition commits to the words it wrote a
 // cycle earlier, long evicted by then).  Threads i0 = 0..n-1 share it;
 // prefetches are hints and change no data.
+// L2 prefetch of what the CTA's item of major stage ms reads first, when
+// that stage assigns items statically: the global-read source table of its
+// first partition, the head of its script (metadata, global-read section,
+// the first two chunks) and the previous-cycle state rows `prev` its commit
+// reads (a partition commits to the words it wrote a cycle earlier, long
+// evicted by then).  Addresses come from the per-launch item table, so no
+// load waits.  Threads i0 = 0..n-1 share it; prefetches are hints and change
+// no data.
 template <int NL>
-__device__ void prefetch_item_l2(const BatchParams &P, unsigned ms, const uint32_t *prev,
-                                 uint32_t i0, uint32_t n) {
-  const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
-                                     : P.num_blocks;
-  const uint32_t per = P.lanes / NL;
-  if ((size_t)nblk * per > gridDim.x || blockIdx.x >= nblk * per) return;
-  const uint32_t bi = blockIdx.x / per;
-  const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
-  const size_t e = (size_t)ms * P.num_blocks + blk;
-  const uint32_t *script = P.blocks_data + P.blocks_start[e];
-  const uint32_t *gr = P.gr_sources + (size_t)P.part_base[e] * 8192;
-  // the script window ends at the end of the script data
-  const size_t left = P.blocks_start[(size_t)P.num_major_stages * P.num_blocks] - P.blocks_start[e];
+__device__ void prefetch_item_l2(const BatchParams &P, const Shared &sh, unsigned ms,
+                                 const uint32_t *prev, uint32_t i0, uint32_t n) {
+  const size_t so = sh.st_off[ms];
+  if (so == ~(size_t)0) return;
+  const uint32_t *script = P.blocks_data + so;
+  const uint32_t *gr = P.gr_sources + (size_t)sh.st_pid[ms] * 8192;
+  const size_t left = sh.script_words - so;  // the window ends with the script data
   constexpr uint32_t GR_LINES = 8192 / 32;                  // 128-byte lines
   constexpr size_t WINDOW = 256 + 512 * 8 + 2 * STAGE_WORDS;
   const uint32_t script_lines = (uint32_t)((left < WINDOW ? left : WINDOW) / 32);
-  for (uint32_t l = i0; l < GR_LINES + script_lines; l += n)
-    prefetch_l2(l < GR_LINES ? gr + 32 * l : script + 32 * (l - GR_LINES));
   // commit rows of the first partition: signals [io_off*32, +num_ios*32)
   // of the item's lane pair, contiguous in the interleaved layout
-  const uint32_t ns = script[0], num_ios = script[2], io_off = script[3];
-  if (ns == 0) return;
+  const uint32_t per = P.lanes / NL;
   const uint32_t lane0 = NL * (blockIdx.x % per);
-  const size_t w0 = phys(P, lane0 & ~1u, (size_t)io_off * 32);
-  const uint32_t lines = num_ios * (P.xhalf ? 4 : 2);  // 32 signals x 16 or 8 bytes
-  for (uint32_t l = i0; l < lines; l += n) prefetch_l2(prev + w0 + 32 * (size_t)l);
+  const size_t w0 = phys(P, lane0 & ~1u, (size_t)sh.st_io[ms] * 32);
+  const uint32_t rows = sh.st_nio[ms] * (P.xhalf ? 4 : 2);  // 32 signals x 16 or 8 bytes
+  for (uint32_t l = i0; l < GR_LINES + script_lines + rows; l += n) {
+    if (l < GR_LINES)
+      prefetch_l2(gr + 32 * l);
+    else if (l < GR_LINES + script_lines)
+      prefetch_l2(script + 32 * (l - GR_LINES));
+    else
+      prefetch_l2(prev + w0 + 32 * (size_t)(l - GR_LINES - script_lines));
+  }
 }
 
 // NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
@@ -1051,6 +1069,33 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   }
   for (uint32_t q = t; q < P.wo_slots * 32 * (uint32_t)(WB / 4); q += BT)
     reinterpret_cast<uint32_t *>(WO)[q] = 0;
+  // item table: thread ms resolves major stage ms
+  if (t == 0) sh.script_words = P.blocks_start[(size_t)P.num_major_stages * P.num_blocks];
+  if ((unsigned)t < P.num_major_stages) {
+    const uint32_t nblk = P.block_list ? P.block_list_start[t + 1] - P.block_list_start[t]
+                                       : P.num_blocks;
+    const uint32_t per = P.lanes / NL;
+    const uint32_t items = nblk * per;
+    size_t so = ~(size_t)0;
+    uint32_t pid = 0, nio = 0, io = 0;
+    if (items <= gridDim.x && blockIdx.x < items) {
+      const uint32_t bi = blockIdx.x / per;
+      const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[t] + bi] : bi;
+      const size_t e = (size_t)t * P.num_blocks + blk;
+      so = P.blocks_start[e];
+      pid = P.part_base[e];
+      const uint32_t *sc = P.blocks_data + so;
+      if (sc[0]) {
+        nio = sc[2];
+        io = sc[3];
+      }
+    }
+    sh.st_items[t] = items;
+    sh.st_off[t] = so;
+    sh.st_pid[t] = pid;
+    sh.st_nio[t] = nio;
+    sh.st_io[t] = io;
+  }
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
@@ -1080,10 +1125,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       }
     }
     for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
-      const uint32_t nblk = P.block_list ? P.block_list_start[ms + 1] - P.block_list_start[ms]
-                                         : P.num_blocks;
       const uint32_t per = P.lanes / NL;  // items per block
-      const uint32_t items = nblk * per;
+      const uint32_t items = sh.st_items[ms];
       // at most one item per CTA: item = CTA index (so the CTA knows its
       // next item early and can prefetch it); otherwise tickets
       const bool dyn = items > gridDim.x;
@@ -1103,9 +1146,16 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         const uint32_t tk = sh.ticket;
         if (tk >= items) break;
         const uint32_t bi = tk / per, lane = tk % per;
-        const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
-        const uint32_t *script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
-        const uint32_t pid0 = P.part_base[(size_t)ms * P.num_blocks + blk];
+        const uint32_t *script;
+        uint32_t pid0;
+        if (!dyn) {  // the item table holds this CTA's item
+          script = P.blocks_data + sh.st_off[ms];
+          pid0 = sh.st_pid[ms];
+        } else {
+          const uint32_t blk = P.block_list ? P.block_list[P.block_list_start[ms] + bi] : bi;
+          script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
+          pid0 = P.part_base[(size_t)ms * P.num_blocks + blk];
+        }
         if constexpr (NL == 2)
           run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
                     uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next);
@@ -1125,7 +1175,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         // the next stage's previous-cycle snapshot: `in`, or at the end of
         // the cycle this cycle's `out`
         if (ms + 1 < P.num_major_stages || c + 1 < P.num_cycles)
-          prefetch_item_l2<NL>(P, ms2, ms + 1 < P.num_major_stages ? in : out, t - 32, BT - 32);
+          prefetch_item_l2<NL>(P, sh, ms2, ms + 1 < P.num_major_stages ? in : out, t - 32,
+                               BT - 32);
       }
       if (t == 0) {
         unsigned gen = ld_acquire(&g_bar_gen[P.slot]);
