@@ -32,7 +32,26 @@ namespace jqk {
 constexpr int BT = 512;  // threads per CTA
 constexpr uint32_t CHUNK_BYTES = STAGE_WORDS * 4;
 
-static __device__ unsigned int g_ticket[BAR_SLOTS];
+// Grid-barrier arrivals and work tickets of the batched kernel: 64-bit and
+// monotonic within a launch (never reset between major stages), so the
+// last CTA to arrive releases the others with its own atomic.
+static __device__ unsigned long long g_bcount[BAR_SLOTS];
+static __device__ unsigned long long g_bticket[BAR_SLOTS];
+
+__device__ __forceinline__ unsigned long long atom_add_acq_rel(unsigned long long *p,
+                                                                unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;"
+               : "=l"(old)
+               : "l"(p), "l"(v)
+               : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
 // Global-read source table sentinels (jq_batched_prepare).
 constexpr uint32_t GR_EMPTY = 0xffffffffu;  // needed, no source: stored as 0
 constexpr uint32_t GR_SKIP = 0xfffffffeu;   // not needed by any gather
@@ -195,7 +214,7 @@ template <bool DS>
 __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, uint32_t *chunks,
                          uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                          const uint32_t *in, uint32_t *out, uint32_t lane, uint32_t pid0,
-                         bool &failed, uint32_t &next_ticket, bool &have_next) {
+                         bool &failed, unsigned long long &next_ticket, bool &have_next) {
   const int t = threadIdx.x;
   // the lane's words: with xhalf (v, x) pairs at 4 * (pair * V + s) + 2 * odd
   // (X-capable partitions always run in the quad layout), else values at
@@ -551,7 +570,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         // the item's last commit: take the next work ticket now, so its
         // latency overlaps the commit
         if (t == 0 && is_last && sh.dyn) {
-          next_ticket = atomicAdd(&g_ticket[P.slot], 1u);
+          next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
           have_next = true;
         }
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
@@ -637,7 +656,7 @@ __device__ __forceinline__ uint4 shfl4_xor(uint4 v, uint32_t m) {
 __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO, uint32_t *chunks,
                           uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                           const uint32_t *in, uint32_t *out, uint32_t lp, uint32_t pid0,
-                          bool &failed, uint32_t &next_ticket, bool &have_next) {
+                          bool &failed, unsigned long long &next_ticket, bool &have_next) {
   const int t = threadIdx.x;
   // the pair's words: quads (v0, x0, v1, x1) at 4 * (lp * V + s) with
   // xhalf, else (v0, v1) at 2 * (lp * sig + s)
@@ -936,7 +955,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         // ---------------- clock-enable permutation and commit, both lane words
         JQ_FAIL_IF(!ok)
         if (t == 0 && is_last && sh.dyn) {
-          next_ticket = atomicAdd(&g_ticket[P.slot], 1u);
+          next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
           have_next = true;
         }
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
@@ -1099,6 +1118,9 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
+  // thread 0: arrival count that completes the next grid barrier, and the
+  // first ticket of the current major stage
+  unsigned long long bar_target = 0, ticket_base = 0;
   const size_t snap = P.sig_per_snap * P.lanes;  // lane-major record snapshot
 
   for (size_t c = 0; c < P.num_cycles; ++c) {
@@ -1130,15 +1152,18 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       // at most one item per CTA: item = CTA index (so the CTA knows its
       // next item early and can prefetch it); otherwise tickets
       const bool dyn = items > gridDim.x;
-      uint32_t next_ticket = 0;
+      unsigned long long next_ticket = 0;
       bool have_next = false;
       bool done_static = false;
       for (;;) {
         __syncthreads();
         if (t == 0) {
           sh.dyn = dyn;
-          sh.ticket = !dyn ? (done_static ? items : blockIdx.x)
-                           : have_next ? next_ticket : atomicAdd(&g_ticket[P.slot], 1u);
+          // tickets of a dynamic stage are ticket_base + item
+          const unsigned long long tk =
+              !dyn ? (done_static ? items : blockIdx.x)
+                   : (have_next ? next_ticket : atomicAdd(&g_bticket[P.slot], 1ull)) - ticket_base;
+          sh.ticket = tk < items ? (uint32_t)tk : items;
         }
         __syncthreads();
         have_next = false;
@@ -1167,8 +1192,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
           return;
         }
       }
-      // last arriver re-arms the ticket counter inside the barrier; while
-      // thread 0 waits, warps 1.. prefetch this CTA's next item into L2
+      // grid barrier; while thread 0 waits, warps 1.. prefetch this CTA's
+      // next item into L2
       __syncthreads();
       if (t >= 32) {
         const unsigned ms2 = ms + 1 < P.num_major_stages ? ms + 1 : 0;
@@ -1179,18 +1204,20 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
                                BT - 32);
       }
       if (t == 0) {
-        unsigned gen = ld_acquire(&g_bar_gen[P.slot]);
-        __threadfence();
-        unsigned arrived = atomicAdd(&g_bar_count[P.slot], 1u);
+        // every CTA takes exactly one ticket past the last item of a
+        // dynamic stage, so the next stage's tickets start items + grid on
+        if (dyn) ticket_base += items + gridDim.x;
+        bar_target += gridDim.x;
         int ok = 1;
-        if (arrived == gridDim.x - 1) {
-          g_ticket[P.slot] = 0;
-          g_bar_count[P.slot] = 0;
-          __threadfence();
-          atomicAdd(&g_bar_gen[P.slot], 1u);
-        } else {
+        // release: this CTA's writes (ordered by the CTA barrier above);
+        // acquire: every earlier arrival's writes
+        if (atom_add_acq_rel(&g_bcount[P.slot], 1ull) + 1 < bar_target) {
           uint64_t t0 = clock64();
-          while (ld_acquire(&g_bar_gen[P.slot]) == gen) {
+          while (ld_acquire64(&g_bcount[P.slot]) < bar_target) {
+            if (*((volatile int *)&g_status[P.slot]) != 0) {
+              ok = 0;
+              break;
+            }
             __nanosleep(64);
             if ((uint64_t)(clock64() - t0) > P.timeout) {
               ok = 0;
@@ -1199,7 +1226,6 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
             }
           }
         }
-        if (ok && *((volatile int *)&g_status[P.slot]) != 0) ok = 0;
         sh.ok = ok;
       }
       __syncthreads();
@@ -1612,8 +1638,8 @@ __global__ void jq_batched_pack_kernel(const uint32_t *lm, uint32_t *st, uint32_
 // Re-arms one slot's barrier, ticket and status before a launch.  A kernel
 // (not a host copy) so the reset is captured in CUDA graphs with the launch.
 __global__ void jq_batched_reset_kernel(int slot) {
-  g_bar_count[slot] = 0;
-  g_ticket[slot] = 0;
+  g_bcount[slot] = 0;
+  g_bticket[slot] = 0;
   g_status[slot] = 0;
 }
 
