@@ -17,17 +17,21 @@ def per_stream_states(kind, s, cycles, streams, x_init):
     return np.stack(out)  # (S, cycles+1, eff)
 
 
-@pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots,per_item", [
-    ("tiny", 8, (5,), False, 1, None, 0),
-    ("sram", 16, (8,), True, 2, None, 0),     # lane pairs
-    ("sram", 16, (8,), True, 2, None, 1),     # single lanes, double-buffered tree
-    ("sram", 16, (8,), True, 1, 256, 0),      # single-buffered tree state
-    ("sram", 16, (8,), True, 2, 256, 0),      # lane pairs do not fit: single lanes
-    ("tiny", 8, (5,), False, 4, None, 2),
-    ("soc_mini", 148, (20, 40, 60), True, 1, None, 0),
-    ("soc_mini", 148, (20, 40, 60), True, 2, None, 0),
+@pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots,per_item,grid", [
+    ("tiny", 8, (5,), False, 1, None, 0, 0),
+    ("sram", 16, (8,), True, 2, None, 0, 0),     # lane pairs
+    ("sram", 16, (8,), True, 2, None, 1, 0),     # single lanes, double-buffered tree
+    ("sram", 16, (8,), True, 1, 256, 0, 0),      # single-buffered tree state
+    ("sram", 16, (8,), True, 2, 256, 0, 0),      # lane pairs do not fit: single lanes
+    ("tiny", 8, (5,), False, 4, None, 2, 0),
+    ("soc_mini", 148, (20, 40, 60), True, 1, None, 0, 0),
+    ("soc_mini", 148, (20, 40, 60), True, 2, None, 0, 0),
+    # fewer CTAs than items: work tickets instead of one item per CTA
+    ("soc_mini", 148, (20, 40, 60), True, 2, None, 0, 5),
+    ("sram", 16, (8,), True, 2, None, 1, 3),
 ])
-def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slots, per_item):
+def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slots, per_item,
+                                           grid):
     s = cases.script(kind, nb, split, xprop=xprop)
     cycles = 10
     S = 32 * lanes
@@ -44,7 +48,8 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slo
         want[k] = st.reshape(cycles + 1, eff)
         wsram.append(sram)
     # batched
-    B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots, lanes_per_item=per_item)
+    B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots, lanes_per_item=per_item,
+                           grid=grid)
     bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
     B.load_state(bt[0])
     B.reset_sram()
