@@ -33,20 +33,10 @@ constexpr int BT = 512;  // threads per CTA
 constexpr uint32_t CHUNK_BYTES = STAGE_WORDS * 4;
 
 // Grid-barrier arrivals and work tickets of the batched kernel: 64-bit and
-// monotonic within a launch (never reset between major stages), so the
-// last CTA to arrive releases the others with its own atomic.
+// monotonic within a launch (never reset between major stages).
 static __device__ unsigned long long g_bcount[BAR_SLOTS];
 static __device__ unsigned long long g_bticket[BAR_SLOTS];
 
-__device__ __forceinline__ unsigned long long atom_add_acq_rel(unsigned long long *p,
-                                                                unsigned long long v) {
-  unsigned long long old;
-  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;"
-               : "=l"(old)
-               : "l"(p), "l"(v)
-               : "memory");
-  return old;
-}
 __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -194,6 +184,53 @@ struct Shared {
   uint32_t st_io[MAX_MAJOR_STAGES];
   size_t script_words;  // blocks_start[num_major_stages * num_blocks]
 };
+
+// Grid barrier between major stages, split in two so a CTA can load its
+// next item's script data between arriving and waiting.  The arrival count
+// is 64-bit and monotonic within a launch (the target grows by the grid each
+// barrier).  Arrive: a release reduction (this CTA's writes, ordered by the
+// CTA barrier, become visible before the count moves), which thread 0 does
+// not wait for.  Wait: thread 0 polls the count with acquire loads until it
+// reaches the target, and the error status; the other warps run
+// `others(i, n)` (i = 0..n-1) meanwhile.  The CTA learns the outcome; false
+// when the barrier failed.
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.L2 [%0];" ::"l"(p));
+}
+
+__device__ __forceinline__ void grid_arrive(const BatchParams &P, unsigned long long &bar_target) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bar_target += gridDim.x;
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(&g_bcount[P.slot]) : "memory");
+  }
+}
+
+template <class F>
+__device__ bool grid_wait(const BatchParams &P, Shared &sh, unsigned long long bar_target,
+                          F &&others) {
+  const int t = threadIdx.x;
+  if (t >= 32) others((uint32_t)t - 32, (uint32_t)BT - 32);
+  if (t == 0) {
+    int ok = 1;
+    uint64_t t0 = clock64();
+    while (ld_acquire64(&g_bcount[P.slot]) < bar_target) {
+      if (*((volatile int *)&g_status[P.slot]) != 0) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+      if ((uint64_t)(clock64() - t0) > P.timeout) {
+        ok = 0;
+        atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
+        break;
+      }
+    }
+    sh.ok = ok;
+  }
+  __syncthreads();
+  return sh.ok != 0;
+}
 
 // One (block, lane) work item: the block's partition list for one lane word.
 // Tree state and writeouts hold (value, X) pairs so one shared-memory access
@@ -656,7 +693,8 @@ __device__ __forceinline__ uint4 shfl4_xor(uint4 v, uint32_t m) {
 __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO, uint32_t *chunks,
                           uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                           const uint32_t *in, uint32_t *out, uint32_t lp, uint32_t pid0,
-                          bool &failed, unsigned long long &next_ticket, bool &have_next) {
+                          bool &failed, unsigned long long &next_ticket, bool &have_next,
+                          bool &pending, unsigned long long &bar_target) {
   const int t = threadIdx.x;
   // the pair's words: quads (v0, x0, v1, x1) at 4 * (lp * V + s) with
   // xhalf, else (v0, v1) at 2 * (lp * sig + s)
@@ -686,6 +724,22 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     if (t == 0) {
       mbar_expect_tx(&sh.bar[0], CHUNK_BYTES);
       tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
+    }
+    // the wait of the grid barrier that ends the previous major stage (the
+    // CTA arrived before this item), deferred to here so the metadata,
+    // global-read sources and chunk 0 (script data, never written) are on
+    // their way meanwhile; the waiting warps prefetch the commit rows
+    if (pending) {
+      pending = false;
+      const uint32_t *rows = in + pair_base + (((size_t)io_off * 32) << (P.xhalf ? 2 : 1));
+      const uint32_t nl = num_ios * (P.xhalf ? 4 : 2);  // 128-byte lines
+      if (!grid_wait(P, sh, bar_target, [&](uint32_t i0, uint32_t n) {
+            for (uint32_t l = i0; l < nl; l += n) prefetch_l2(rows + 32 * (size_t)l);
+          })) {
+        failed = true;
+        if (t == 0) mbar_wait(&sh.bar[0], uses0 & 1u, P.timeout);
+        return;
+      }
     }
     // ---- global read, both lane words, in two halves of 8 positions
 #pragma unroll
@@ -1024,9 +1078,6 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
 #undef JQ_FAIL_IF
 #undef JQ_HOOKS_COMPACT
 
-__device__ __forceinline__ void prefetch_l2(const void *p) {
-  asm volatile("prefetch.L2 [%0];" ::"l"(p));
-}
 
 // L2 prefetch of what the CTA's item of major stage ms reads first, when
 // that stage assigns items statically (at most one per CTA): the global-read
@@ -1122,6 +1173,11 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   // first ticket of the current major stage
   unsigned long long bar_target = 0, ticket_base = 0;
   const size_t snap = P.sig_per_snap * P.lanes;  // lane-major record snapshot
+  // Lane-pair items take over the barrier that ends the previous major
+  // stage (see run_item2); `pending` marks one owed.
+  constexpr bool DEFER = NL == 2;
+  bool pending = false;
+  auto no_prefetch = [](uint32_t, uint32_t) {};
 
   for (size_t c = 0; c < P.num_cycles; ++c) {
     const uint32_t *in = (c & 1) ? P.state_b : P.state_a;
@@ -1152,6 +1208,10 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       // at most one item per CTA: item = CTA index (so the CTA knows its
       // next item early and can prefetch it); otherwise tickets
       const bool dyn = items > gridDim.x;
+      if (pending && !(DEFER && !dyn && blockIdx.x < items)) {  // no item here to take it
+        pending = false;
+        if (!grid_wait(P, sh, bar_target, no_prefetch)) return;
+      }
       unsigned long long next_ticket = 0;
       bool have_next = false;
       bool done_static = false;
@@ -1183,7 +1243,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         }
         if constexpr (NL == 2)
           run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
-                    uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next);
+                    uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
+                    pending, bar_target);
         else
           run_item<DS>(P, sh, reinterpret_cast<uint2 *>(S), reinterpret_cast<uint2 *>(WO), chunks,
                        uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next);
@@ -1192,44 +1253,28 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
           return;
         }
       }
-      // grid barrier; while thread 0 waits, warps 1.. prefetch this CTA's
-      // next item into L2
-      __syncthreads();
-      if (t >= 32) {
+      if (pending) {  // the item had no partition to take it
+        pending = false;
+        if (!grid_wait(P, sh, bar_target, no_prefetch)) return;
+      }
+      // every CTA takes exactly one ticket past the last item of a dynamic
+      // stage, so the next stage's tickets start items + grid on
+      if (t == 0 && dyn) ticket_base += items + gridDim.x;
+      grid_arrive(P, bar_target);
+      if (DEFER && ms + 1 < P.num_major_stages) {
+        pending = true;  // the wait comes with the next item
+      } else {
+        // grid barrier; while thread 0 waits, warps 1.. prefetch this CTA's
+        // next item into L2 (the next stage's previous-cycle snapshot: `in`,
+        // or at the end of the cycle this cycle's `out`)
         const unsigned ms2 = ms + 1 < P.num_major_stages ? ms + 1 : 0;
-        // the next stage's previous-cycle snapshot: `in`, or at the end of
-        // the cycle this cycle's `out`
-        if (ms + 1 < P.num_major_stages || c + 1 < P.num_cycles)
-          prefetch_item_l2<NL>(P, sh, ms2, ms + 1 < P.num_major_stages ? in : out, t - 32,
-                               BT - 32);
+        const bool more = ms + 1 < P.num_major_stages || c + 1 < P.num_cycles;
+        const uint32_t *prev = ms + 1 < P.num_major_stages ? in : out;
+        if (!grid_wait(P, sh, bar_target, [&](uint32_t i0, uint32_t n) {
+              if (more) prefetch_item_l2<NL>(P, sh, ms2, prev, i0, n);
+            }))
+          return;
       }
-      if (t == 0) {
-        // every CTA takes exactly one ticket past the last item of a
-        // dynamic stage, so the next stage's tickets start items + grid on
-        if (dyn) ticket_base += items + gridDim.x;
-        bar_target += gridDim.x;
-        int ok = 1;
-        // release: this CTA's writes (ordered by the CTA barrier above);
-        // acquire: every earlier arrival's writes
-        if (atom_add_acq_rel(&g_bcount[P.slot], 1ull) + 1 < bar_target) {
-          uint64_t t0 = clock64();
-          while (ld_acquire64(&g_bcount[P.slot]) < bar_target) {
-            if (*((volatile int *)&g_status[P.slot]) != 0) {
-              ok = 0;
-              break;
-            }
-            __nanosleep(64);
-            if ((uint64_t)(clock64() - t0) > P.timeout) {
-              ok = 0;
-              atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
-              break;
-            }
-          }
-        }
-        sh.ok = ok;
-      }
-      __syncthreads();
-      if (!sh.ok) return;
     }
     // record outputs of this cycle
     for (size_t q = (size_t)blockIdx.x * BT + t; q < (size_t)P.n_po * P.lanes;
