@@ -185,6 +185,13 @@ struct Shared {
   size_t script_words;  // blocks_start[num_major_stages * num_blocks]
 };
 
+// Bytes to copy of chunk k of a partition: compact partitions list the
+// used prefix of each chunk in metadata words 11 + k (0: the whole chunk).
+__device__ __forceinline__ uint32_t chunk_bytes(const Shared &sh, uint32_t k) {
+  const uint32_t b = (sh.meta[10] & 1u) && k < 116 ? sh.meta[11 + k] : 0u;
+  return b ? b : CHUNK_BYTES;
+}
+
 // Grid barrier between major stages, split in two so a CTA can load its
 // next item's script data between arriving and waiting.  The arrival count
 // is 64-bit and monotonic within a launch (the target grows by the grid each
@@ -291,8 +298,9 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
 
     // chunk 0 -> buffer 0 (the previous item/partition finished with both)
     if (t == 0) {
-      mbar_expect_tx(&sh.bar[0], CHUNK_BYTES);
-      tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
+      const uint32_t nb = chunk_bytes(sh, 0);
+      mbar_expect_tx(&sh.bar[0], nb);
+      tma_load_1d(chunks, ch0, nb, &sh.bar[0]);
     }
 
     // ---- global read into tree buffer 0.  The source signal of every
@@ -351,9 +359,10 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
       // The other buffer's last reader finished before the final barrier of
       // the previous chunk, so the next chunk can be issued right away.
       if (t == 0 && ci + 1 < nchunks) {
-        mbar_expect_tx(&sh.bar[b ^ 1], CHUNK_BYTES);
         const uint32_t nxt = (!has_sram && ci + 1 == ns) ? ns + 1 : ci + 1;  // script chunk
-        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, CHUNK_BYTES,
+        const uint32_t nb = chunk_bytes(sh, nxt);
+        mbar_expect_tx(&sh.bar[b ^ 1], nb);
+        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, nb,
                     &sh.bar[b ^ 1]);
       }
       uint32_t &uses = b ? uses1 : uses0;
@@ -381,10 +390,10 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         // reads the previous region and writes its own, disjoint one, so one
         // barrier per stage (a stage-0 region that overlaps the global read
         // is computed in full before it is stored)
-        const uint32_t n = ok ? C[4096] : 0u, base = ok ? C[4097] : 0u;
+        const uint32_t n = ok ? C[0] : 0u, base = ok ? C[1] : 0u;
 #define JQ_COMPACT_EVAL(i, r)                                                              \
   {                                                                                        \
-    const uint32_t en = C[i];                                                              \
+    const uint32_t en = C[4 + (i)];                                                              \
     const uint2 ga = ((en >> 29) & 1u) ? make_uint2(0, 0) : Sb0[en & 8191u];               \
     const uint2 gb = ((en >> 30) & 1u) ? make_uint2(0, 0) : Sb0[(en >> 13) & 8191u];       \
     xand(ga.x, ga.y, gb.x, gb.y, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u),           \
@@ -392,7 +401,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
   }
         // slots below ov (stage 0 only, at most 4 * BT) lie over the global
         // read: held in registers until every thread has gathered
-        const uint32_t ov = ok ? C[4098] : 0u;
+        const uint32_t ov = ok ? C[2] : 0u;
         uint2 h[4] = {make_uint2(0, 0), make_uint2(0, 0), make_uint2(0, 0), make_uint2(0, 0)};
         if (ok) {
           if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
@@ -722,8 +731,9 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     const bool has_sram = (num_srams | num_dup) != 0;
     const uint32_t nchunks = ns + (has_sram ? 2 : 1);
     if (t == 0) {
-      mbar_expect_tx(&sh.bar[0], CHUNK_BYTES);
-      tma_load_1d(chunks, ch0, CHUNK_BYTES, &sh.bar[0]);
+      const uint32_t nb = chunk_bytes(sh, 0);
+      mbar_expect_tx(&sh.bar[0], nb);
+      tma_load_1d(chunks, ch0, nb, &sh.bar[0]);
     }
     // the wait of the grid barrier that ends the previous major stage (the
     // CTA arrived before this item), deferred to here so the metadata,
@@ -786,9 +796,10 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       uint32_t *C = chunks + b * STAGE_WORDS;
       if (ci == 0) __syncthreads();  // global read complete
       if (t == 0 && ci + 1 < nchunks) {
-        mbar_expect_tx(&sh.bar[b ^ 1], CHUNK_BYTES);
         const uint32_t nxt = (!has_sram && ci + 1 == ns) ? ns + 1 : ci + 1;
-        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, CHUNK_BYTES,
+        const uint32_t nb = chunk_bytes(sh, nxt);
+        mbar_expect_tx(&sh.bar[b ^ 1], nb);
+        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, nb,
                     &sh.bar[b ^ 1]);
       }
       uint32_t &uses = b ? uses1 : uses0;
@@ -809,15 +820,15 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       if (compact && ci == ns && ok) JQ_HOOKS_COMPACT(ns - 1, prev_base)
       if (ci < ns && compact) {
         // ---------------- compact stage ci (see run_item)
-        const uint32_t n = ok ? C[4096] : 0u, base = ok ? C[4097] : 0u;
+        const uint32_t n = ok ? C[0] : 0u, base = ok ? C[1] : 0u;
 #define JQ_COMPACT_EVAL(i, r)                                                                \
   {                                                                                          \
-    const uint32_t en = C[i];                                                                \
+    const uint32_t en = C[4 + (i)];                                                                \
     const uint4 ga = ((en >> 29) & 1u) ? make_uint4(0, 0, 0, 0) : S[en & 8191u];             \
     const uint4 gb = ((en >> 30) & 1u) ? make_uint4(0, 0, 0, 0) : S[(en >> 13) & 8191u];     \
     r = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u), 0u - ((en >> 28) & 1u)); \
   }
-        const uint32_t ov = ok ? C[4098] : 0u;  // held slots (stage 0)
+        const uint32_t ov = ok ? C[2] : 0u;  // held slots (stage 0)
         uint4 h[4] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
         if (ok) {
           if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
@@ -1537,10 +1548,11 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     // reaches into it, the first `ov` slots of stage 0 (at most 4 per
     // thread) are held until every thread has read the global read.  The
     // chunk becomes one word per slot: source words a | b << 13, flags xa <<
-    // 26, xb << 27, ob << 28, zero-source flags << 29 (a) and << 30 (b);
-    // words 4096, 4097, 4098 hold the slot count, the region's first word
-    // and ov.  Hooks are rewritten to (stage << 8) | block.  Metadata word 10
-    // bit 0 marks the form.
+    // 26, xb << 27, ob << 28, zero-source flags << 29 (a) and << 30 (b),
+    // after a header of four words: the slot count, the region's first word,
+    // ov and 0.  Hooks are rewritten to (stage << 8) | block.  Metadata word
+    // 10 bit 0 marks the form, words 11 + k the bytes of chunk k to copy
+    // (header and slot words; 0 = the whole chunk).
     bool compact = all_flat && ns <= COMPACT_MAX_STAGES;
     if (compact) {
       for (uint32_t ci = 0; ci < ns; ++ci) {
@@ -1606,13 +1618,16 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
           const uint32_t wa = (ci > 0 && sa == 0) ? 0xffffu : ps.slot_prev[sa];
           const uint32_t wb = (ob || (ci > 0 && sb == 0)) ? 0xffffu : ps.slot_prev[sb];
           const uint32_t za = wa == 0xffffu, zb = wb == 0xffffu;
-          D[i] = (za ? 0u : wa) | ((zb ? 0u : wb) << 13) | (xa << 26) | (xb << 27) | (ob << 28) |
+          D[4 + i] = (za ? 0u : wa) | ((zb ? 0u : wb) << 13) | (xa << 26) | (xb << 27) | (ob << 28) |
                  (za << 29) | (zb << 30);
         }
         if (t == 0) {
-          D[4096] = n;
-          D[4097] = base;
-          D[4098] = ov;
+          D[0] = n;
+          D[1] = base;
+          D[2] = ov;
+          D[3] = 0;
+          // copy size of this chunk: the header and the slot words
+          dst[off + 11 + ci] = ((4 + n) * 4 + 15) & ~15u;
         }
         if (t < 128 && 2 * t < nio) {  // meta word 128 + t: hooks of slots 2t, 2t+1
           uint32_t w = dst[off + 128 + t];
@@ -1631,7 +1646,10 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         __syncthreads();
       }
     }
-    if (t == 0) dst[off + 10] = compact ? 1u : 0u;
+    if (t == 0) {
+      dst[off + 10] = compact ? 1u : 0u;
+      if (compact) dst[off + 11 + ns] = dst[off + 12 + ns] = 0;  // SRAM, commit: whole
+    }
     for (uint32_t ci = ns; ci < ns + 2; ++ci) {
       const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
       uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
