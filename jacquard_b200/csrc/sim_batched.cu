@@ -1132,6 +1132,30 @@ __device__ void prefetch_item_l2(const BatchParams &P, const Shared &sh, unsigne
   }
 }
 
+// L2 prefetch of the state words the global read of the CTA's item of major
+// stage ms takes from the previous-cycle snapshot `prev` (sources without the
+// staged bit), from its first partition's compacted source row.  The loads
+// of the row wait, so only CTAs with time to spare call it.
+template <int NL>
+__device__ void prefetch_global_read_l2(const BatchParams &P, const Shared &sh, unsigned ms,
+                                        const uint32_t *prev, uint32_t i0, uint32_t n) {
+  if (sh.st_off[ms] == ~(size_t)0) return;
+  const uint32_t *row = P.gr_sources + (size_t)sh.st_pid[ms] * 8192;
+  const uint32_t per = P.lanes / NL;
+  const uint32_t lane0 = NL * (blockIdx.x % per);
+  const size_t pb = phys(P, lane0 & ~1u, 0);  // the lane pair's word of signal 0
+  const uint32_t sh2 = P.xhalf ? 2 : 1;
+  constexpr int K = 18;  // 18 * 480 >= 8192 slots: one round of row loads
+  for (uint32_t q0 = i0; q0 < 8192; q0 += K * n) {
+    uint32_t ev[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) ev[k] = q0 + k * n < 8192 ? __ldg(row + q0 + k * n) : GR_SKIP;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (ev[k] < 0x80000000u) prefetch_l2(prev + pb + ((size_t)ev[k] << sh2));
+  }
+}
+
 // NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
 template <bool DS, int NL>
 __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
@@ -1281,8 +1305,13 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         const unsigned ms2 = ms + 1 < P.num_major_stages ? ms + 1 : 0;
         const bool more = ms + 1 < P.num_major_stages || c + 1 < P.num_cycles;
         const uint32_t *prev = ms + 1 < P.num_major_stages ? in : out;
+        // a CTA that had no item in this stage waits long (the stage's items
+        // run meanwhile): it also prefetches the state words its next item's
+        // global read takes from `prev`
+        const bool idle = blockIdx.x >= items;
         if (!grid_wait(P, sh, bar_target, [&](uint32_t i0, uint32_t n) {
               if (more) prefetch_item_l2<NL>(P, sh, ms2, prev, i0, n);
+              if (more && idle) prefetch_global_read_l2<NL>(P, sh, ms2, prev, i0, n);
             }))
           return;
       }
