@@ -167,6 +167,20 @@ __device__ __forceinline__ size_t phys(const BatchParams &P, uint32_t l, size_t 
 
 constexpr uint32_t MAX_MAJOR_STAGES = 32;  // jq_simulate_batched's limit
 
+// 32x32 bit transpose across a warp: lane l holds row l on entry and
+// column l on return (bit r of the result = bit l of lane r's input), by
+// swapping off-diagonal blocks of 16, 8, 4, 2 and 1 bits.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t m = 0x0000ffffu;
+#pragma unroll
+  for (int j = 16; j; j >>= 1, m ^= m << j) {
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? (x & ~m) | ((y & ~m) >> j) : (x & m) | ((y & m) << j);
+  }
+  return x;
+}
+
 struct Shared {
   uint32_t meta[256];
   uint64_t bar[2];
@@ -570,19 +584,13 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         const int warp = t >> 5, ln = t & 31;
         for (uint32_t i = warp; i < num_srams; i += BT / 32) {
           const uint2 *Aw = St + (4 * i) * 32;
-          uint32_t ra = 0, wa = 0, en = 0, data = 0, datax = 0;
-#pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            ra |= ((Aw[k].x >> ln) & 1u) << k;
-            wa |= ((Aw[16 + k].x >> ln) & 1u) << k;
-          }
-#pragma unroll 8
-          for (int k = 0; k < 32; ++k) {
-            en |= ((Aw[32 + k].x >> ln) & 1u) << k;
-            const uint2 dk = Aw[64 + k];
-            data |= ((dk.x >> ln) & 1u) << k;
-            datax |= ((dk.y >> ln) & 1u) << k;
-          }
+          // staged rows (read address 0..15, write address 16..31, write
+          // enable 32..63, data 64..95) to per-stream bits by warp transposes
+          const uint32_t addr = warp_transpose32(Aw[ln].x);
+          const uint32_t ra = addr & 0xffffu, wa = addr >> 16;
+          const uint32_t en = warp_transpose32(Aw[32 + ln].x);
+          const uint2 dk = Aw[64 + ln];
+          const uint32_t data = warp_transpose32(dk.x), datax = warp_transpose32(dk.y);
           const size_t stream = (size_t)lane * 32 + ln;
           uint32_t *ram = P.sram + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS;
           const uint32_t r = ldcg(ram + ra), w0 = ldcg(ram + wa);
@@ -599,12 +607,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           if (hx) ramx[wa] = (w0x & ~en) | (datax & en);
           // transpose the 32 streams' read words into 32 signal words
           const uint32_t slotw = (num_ios - num_srams + i) * 32;
-#pragma unroll 4
-          for (int k = 0; k < 32; ++k) {
-            const uint32_t word = __ballot_sync(0xffffffffu, (r >> k) & 1u);
-            const uint32_t wordx = __ballot_sync(0xffffffffu, (rx >> k) & 1u);
-            if (ln == k) WO[slotw + k] = make_uint2(word, is_x ? wordx : 0u);
-          }
+          WO[slotw + ln] = make_uint2(warp_transpose32(r), is_x ? warp_transpose32(rx) : 0u);
         }
         for (uint32_t q = t; q < num_dup * 32; q += BT)
           WO[(num_ios - num_srams - num_dup) * 32 + q] = St[num_srams * 4 * 32 + q];
@@ -974,19 +977,14 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         for (uint32_t ih = warp; ih < num_srams * 2; ih += BT / 32) {
           const uint32_t i = ih >> 1, hsel = ih & 1;
           const uint32_t *Aw = reinterpret_cast<const uint32_t *>(St + (4 * i) * 32) + 2 * hsel;
-          uint32_t ra = 0, wa = 0, en = 0, data = 0, datax = 0;
-#pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            ra |= ((Aw[4 * k] >> ln) & 1u) << k;
-            wa |= ((Aw[4 * (16 + k)] >> ln) & 1u) << k;
-          }
-#pragma unroll 8
-          for (int k = 0; k < 32; ++k) {
-            en |= ((Aw[4 * (32 + k)] >> ln) & 1u) << k;
-            const uint2 dk = *reinterpret_cast<const uint2 *>(Aw + 4 * (64 + k));
-            data |= ((dk.x >> ln) & 1u) << k;
-            datax |= ((dk.y >> ln) & 1u) << k;
-          }
+          // signal words k of the SRAM's staged rows (read address 0..15,
+          // write address 16..31, write enable 32..63, data 64..95) to the
+          // stream's bits: lane = stream after a warp transpose
+          const uint32_t addr = warp_transpose32(Aw[4 * ln]);
+          const uint32_t ra = addr & 0xffffu, wa = addr >> 16;
+          const uint32_t en = warp_transpose32(Aw[4 * (32 + ln)]);
+          const uint2 dk = *reinterpret_cast<const uint2 *>(Aw + 4 * (64 + ln));
+          const uint32_t data = warp_transpose32(dk.x), datax = warp_transpose32(dk.y);
           const size_t stream = (size_t)(2 * lp + hsel) * 32 + ln;
           uint32_t *ram = P.sram + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS;
           const uint32_t r = ldcg(ram + ra), w0 = ldcg(ram + wa);
@@ -1001,17 +999,12 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           }
           ram[wa] = (w0 & ~en) | (data & en);
           if (hx) ramx[wa] = (w0x & ~en) | (datax & en);
+          // the streams' read words back to 32 signal words (lane = bit)
           const uint32_t slotw = (num_ios - num_srams + i) * 32;
           uint32_t *WOw = reinterpret_cast<uint32_t *>(WO);
-#pragma unroll 4
-          for (int k = 0; k < 32; ++k) {
-            const uint32_t word = __ballot_sync(0xffffffffu, (r >> k) & 1u);
-            const uint32_t wordx = __ballot_sync(0xffffffffu, (rx >> k) & 1u);
-            if (ln == k) {
-              WOw[4 * (slotw + k) + 2 * hsel] = word;
-              WOw[4 * (slotw + k) + 2 * hsel + 1] = is_x ? wordx : 0u;
-            }
-          }
+          const uint32_t word = warp_transpose32(r), wordx = warp_transpose32(rx);
+          *reinterpret_cast<uint2 *>(WOw + 4 * (slotw + ln) + 2 * hsel) =
+              make_uint2(word, is_x ? wordx : 0u);
         }
         for (uint32_t q = t; q < num_dup * 32; q += BT)
           WO[(num_ios - num_srams - num_dup) * 32 + q] = St[num_srams * 4 * 32 + q];
