@@ -1269,6 +1269,14 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
           script = P.blocks_data + P.blocks_start[(size_t)ms * P.num_blocks + blk];
           pid0 = P.part_base[(size_t)ms * P.num_blocks + blk];
         }
+        // the next stage's item: its source row and script head into L2 a
+        // whole stage ahead (hints; the row and script are never written)
+        if (!dyn && ms + 1 < P.num_major_stages && sh.st_off[ms + 1] != ~(size_t)0) {
+          const uint32_t *nrow = P.gr_sources + (size_t)sh.st_pid[ms + 1] * 8192;
+          const uint32_t *nscr = P.blocks_data + sh.st_off[ms + 1];
+          if (t < 256) prefetch_l2(nrow + 32 * t);
+          else if (t < 256 + 48) prefetch_l2(nscr + 32 * (t - 256));  // metadata, chunk 0 head
+        }
         if constexpr (NL == 2)
           run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
                     uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
