@@ -754,7 +754,27 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         return;
       }
     }
-    // ---- global read, both lane words, in two halves of 8 positions
+    // ---- global read, both lane words.  X-capable partitions of the quad
+    // layout copy each slot's 16 bytes straight into shared memory with
+    // cp.async (L2 only, so words other SMs wrote before the barrier are
+    // seen), all 16 slots in flight at once; the others load through
+    // registers in two halves of 8 positions.
+    if (P.xhalf && is_x) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uint32_t ek = e[k];
+        uint4 *dst = &S[sw(t + BT * k)];
+        if (ek < GR_SKIP) {
+          const uint32_t *bp = (ek >> 31) ? out : in;
+          const uint32_t *src = bp + pair_base + ((size_t)(ek & 0x7fffffffu) << 2);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+                       : "memory");
+        } else if (ek == GR_EMPTY) {
+          *dst = make_uint4(0, 0, 0, 0);
+        }
+      }
+      asm volatile("cp.async.wait_all;" ::: "memory");
+    } else {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       uint4 v[8];
@@ -778,6 +798,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
 #pragma unroll
       for (int k = 0; k < 8; ++k)
         if (e[8 * h + k] != GR_SKIP) S[sw(t + BT * (8 * h + k))] = v[k];
+    }
     }
     const uint32_t lane_i = t & 31, warp_i = t >> 5;
     const uint32_t u = residue(t);
