@@ -1,27 +1,31 @@
 // Bit-lane batched interpreter for sm_100a: many independent stimulus streams
 // run the same script in one launch.
 //
-// Layout: a lane word is one u32 holding one signal of 32 streams.  The state
-// is lane-major, T[lane * signals + signal] for L lane words (32*L streams),
-// where `signal` is the bit position of the plain layout (word*32 + bit); the
-// X plane sits at signal offset xoff*32 exactly as in the plain layout.  A
-// work item touches one lane, so its commit writes are contiguous and the
-// signals one global-read mask selects share a 128-byte line.  In this
-// form the boomerang 16-pair bit shuffle becomes a word gather and every tree
-// position evaluates one 32-stream word:
+// Layout: a lane word is one u32 holding one signal of 32 streams, where
+// `signal` is the bit position of the plain layout (word*32 + bit) and the X
+// plane of signal s is signal V + s.  The state interleaves lane pairs: the
+// (value, X) words of both lane words of a pair for one signal are one
+// 16-byte quad (phys() below), so a lane-pair work item reads or commits a
+// signal with one access.  In this form the boomerang 16-pair bit shuffle
+// becomes a word gather and every tree position evaluates one 32-stream word:
 //     v[p] = (v[p+L] ^ xa_p) & ((v[p+2L] ^ xb_p) | ob_p),  L = msb(p)
 // (the plain kernel's level-0 / shared / warp / bit-level tree steps are all
 // this one positional rule).  Semantics per stream are those of the plain
 // interpreter (csrc/kernel_v1_impl.cuh:32-563).
 //
-// Work item = (script block, lane word) for one (cycle, major stage); CTAs
-// take items from a ticket counter (block-major, so the L lane items of one
-// block run back to back and share its script in L2).  Each 20 KB script
-// chunk is staged into shared memory with a TMA bulk copy (cp.async.bulk,
-// mbarrier completion, double-buffered one chunk ahead).  Tree levels 1..4 of
-// a stage stay in registers: thread t owns positions t + 512k, whose
-// children are its own.  Timing arrivals / setup-hold events are handled by
-// the plain interpreter (they do not depend on the stimulus stream).
+// Work item = (script block, lane pair or lane word) for one (cycle, major
+// stage).  When a major stage has no more items than CTAs, CTA i runs item i
+// (a per-launch table in shared memory holds its script offset and first
+// partition); otherwise CTAs take items from a ticket counter.  Major stages
+// are separated by a split grid barrier: arrive after the last commit, wait
+// inside the next item once its script data is requested.  The script is
+// first rewritten by jq_batched_prepare (liveness of tree positions, a
+// thread-major tree form or a compact one-word-per-live-position form,
+// compacted global-read slots).  Each script chunk is staged into shared
+// memory with a TMA bulk copy (cp.async.bulk, mbarrier completion,
+// double-buffered one chunk ahead); the global read copies its slots with
+// cp.async.  Timing arrivals / setup-hold events are handled by the plain
+// interpreter (they do not depend on the stimulus stream).
 #include "sim_common.cuh"
 
 #include <cstdio>
@@ -56,7 +60,7 @@ struct BatchParams {
   size_t sig_per_snap;      // effective words * 32
   int xhalf;                // quad layout: signals [V, 2V) are the X of [0, V)
   size_t vsig;              // V: value signals (sig_per_snap / 2 with xhalf)
-  uint32_t *state_a, *state_b;  // ping-pong snapshots, lane-major
+  uint32_t *state_a, *state_b;  // ping-pong snapshots, interleaved lane pairs (phys())
   const uint32_t *stim;     // [cycle+1][lanes][input_sigs] input values, or null
   size_t input_sigs;        // stimulus signals per lane per cycle
   const uint32_t *input_regions;  // (dst signal, src signal, count) triples or null
