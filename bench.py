@@ -176,10 +176,16 @@ def learned_model():
     return costmodel.packed_from_file(MODEL_PATH)
 
 
-def build_script(d, num_blocks, xprop=True, cost_model=None):
+def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0):
+    """target_parts > 0 cuts each major stage into at most that many
+    partitions of balanced cone size, without merges: the batched kernel
+    then runs every stage as one round of work items, one per CTA (a
+    partition makes lanes / 2 lane-pair items).  Otherwise partitions come
+    from the cone target, merged by the learned rule when a model is given."""
     return d.build_script(num_blocks=num_blocks, level_split=LEVEL_SPLIT, xprop=xprop,
                           target_cone=TARGET_CONE, cost_model=cost_model,
-                          merge_passes=3 if cost_model is not None else 1)
+                          merge_passes=0 if target_parts else (3 if cost_model is not None else 1),
+                          target_parts=target_parts)
 
 
 def algorithmic_bytes_per_cycle(s, lanes=1, arrivals=False):
@@ -305,7 +311,8 @@ def run_mine_batched(args, rank, world):
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
     model = None if args.no_learned else learned_model()
-    s = build_script(d, args.blocks, cost_model=model)
+    s = build_script(d, args.blocks, cost_model=model,
+                     target_parts=args.blocks // max(1, args.lanes // 2))
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
@@ -363,7 +370,8 @@ def run_mine_batched(args, rank, world):
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
-                            partitioner="learned" if model is not None else "heuristic"),
+                            partitioner="balanced: at most %d per major stage"
+                            % (args.blocks // max(1, args.lanes // 2))),
                 script=s, d=d)
 
 

@@ -158,7 +158,10 @@ typedef struct {
                                       per partition, summed over work items
                                       (a lane-pair item counts once) and
                                       cycles (partition order of the script:
-                                      major stage, block, position in block) */
+                                      major stage, block, position in block);
+                                      the grid-barrier wait an item takes
+                                      over from the previous stage is not
+                                      counted */
   const uint32_t *part_base;   /* device: index of the first partition of each
                                   (major stage, block), from jq_batched_prepare */
   const uint32_t *gr_sources;  /* device: global-read sources, from

@@ -80,6 +80,14 @@ typedef struct {
    * predicted kernel time of the merged partition is below the sum of the
    * two; otherwise the stage-count rule is used. */
   const float *cost_model;
+  /* Partitioner: when non-zero, each major stage's endpoints are cut into at
+   * most this many chunks of balanced cone size (the smallest bound on a
+   * chunk's AND count that gives that many) instead of chunks of
+   * target_cone, and merges keep every partition within that bound.  The
+   * batched kernel runs one work item per (partition, lane-word group) per
+   * CTA, so grid / groups partitions per stage keep every stage to one
+   * round of items. */
+  uint32_t target_parts;
 } jqf_build_params;
 
 #define JQF_FEATURES 24

@@ -207,6 +207,7 @@ void *jqf_build_script(void *dp, const jqf_build_params *bp, char *err, size_t e
     if (bp->target_endpoint_bits) po.target_endpoint_bits = bp->target_endpoint_bits;
     po.num_threads = bp->num_threads;
     po.merge_passes = bp->merge_passes;
+    po.target_parts = bp->target_parts;
     CostModel cm;
     std::vector<uint8_t> xp;
     if (bp->cost_model) {

@@ -85,6 +85,10 @@ struct PartitionOptions {
   uint32_t target_endpoint_bits = 2048;
   int num_threads = 0;             // 0 = hardware concurrency
   int merge_passes = 1;
+  // when non-zero, each stage is cut into at most this many chunks of
+  // balanced cone size instead of chunks of target_cone, and merges keep
+  // every partition's cone within the balanced bound
+  uint32_t target_parts = 0;
   // when set, merges are accepted on predicted kernel time instead of the
   // stage-count rule
   const CostModel *cost_model = nullptr;

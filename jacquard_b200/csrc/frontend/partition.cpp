@@ -108,22 +108,16 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
 
   // ---- 2. chunking by cone size / endpoint bits
   std::vector<std::vector<uint32_t>> chunks;
+  uint64_t cone_bound = 0;  // balanced mode: the largest chunk cone allowed
   {
     std::vector<uint32_t> mark(g.num_pins + 1, 0);
     uint32_t gen = 1;
-    std::vector<uint32_t> cur;
-    uint64_t cone = 0, bits = 0;
     std::vector<uint32_t> stk;
-    for (uint32_t e : order) {
-      uint64_t add = 0, eb = 0;
+    // AND gates of endpoint e's cone not yet marked `gen` (marks them)
+    auto grow = [&](uint32_t e) {
+      uint64_t add = 0;
       stk.clear();
-      st.for_each_input(g, e, [&](uint32_t p) { stk.push_back(p); eb++; });
-      if (!cur.empty() && (bits + eb > opt.target_endpoint_bits)) {
-        chunks.push_back(cur);
-        cur.clear();
-        cone = bits = 0;
-        ++gen;
-      }
+      st.for_each_input(g, e, [&](uint32_t p) { stk.push_back(p); });
       while (!stk.empty()) {
         uint32_t u = stk.back();
         stk.pop_back();
@@ -134,17 +128,86 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
         stk.push_back(g.fa[u] >> 1);
         stk.push_back(g.fb[u] >> 1);
       }
-      cur.push_back(e);
-      cone += add;
-      bits += eb;
-      if (cone >= opt.target_cone) {
-        chunks.push_back(cur);
-        cur.clear();
-        cone = bits = 0;
-        ++gen;
+      return add;
+    };
+    auto endpoint_bits = [&](uint32_t e) {
+      uint64_t eb = 0;
+      st.for_each_input(g, e, [&](uint32_t) { eb++; });
+      return eb;
+    };
+    // Balanced: a chunk is closed before the endpoint whose cone would take
+    // it past `bound`, so no chunk of several endpoints exceeds it.  Returns
+    // the number of chunks (stored into `out` when given).
+    auto cut_balanced = [&](uint64_t bound, std::vector<std::vector<uint32_t>> *out) {
+      size_t n = 0;
+      std::vector<uint32_t> cur;
+      uint64_t cone = 0, bits = 0;
+      ++gen;
+      for (uint32_t e : order) {
+        const uint64_t eb = endpoint_bits(e);
+        bool close = !cur.empty() && bits + eb > opt.target_endpoint_bits;
+        uint64_t add = 0;
+        if (!close) {
+          add = grow(e);
+          close = !cur.empty() && cone + add > bound;
+        }
+        if (close) {
+          ++n;
+          if (out) out->push_back(cur);
+          cur.clear();
+          cone = bits = 0;
+          ++gen;
+          add = grow(e);
+        }
+        cur.push_back(e);
+        cone += add;
+        bits += eb;
       }
+      if (!cur.empty()) {
+        ++n;
+        if (out) out->push_back(cur);
+      }
+      ++gen;
+      return n;
+    };
+    if (opt.target_parts) {
+      // the smallest bound that cuts the stage into at most target_parts
+      // chunks (binary search; the whole stage as one chunk is the top)
+      uint64_t lo = 1, hi = 0;
+      ++gen;
+      for (uint32_t e : order) hi += grow(e);
+      hi = std::max<uint64_t>(hi, 1);
+      while (lo < hi) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (cut_balanced(mid, nullptr) <= opt.target_parts) hi = mid;
+        else lo = mid + 1;
+      }
+      cone_bound = lo;
+      cut_balanced(lo, &chunks);
+    } else {
+      std::vector<uint32_t> cur;
+      uint64_t cone = 0, bits = 0;
+      for (uint32_t e : order) {
+        const uint64_t eb = endpoint_bits(e);
+        if (!cur.empty() && (bits + eb > opt.target_endpoint_bits)) {
+          chunks.push_back(cur);
+          cur.clear();
+          cone = bits = 0;
+          ++gen;
+        }
+        const uint64_t add = grow(e);
+        cur.push_back(e);
+        cone += add;
+        bits += eb;
+        if (cone >= opt.target_cone) {
+          chunks.push_back(cur);
+          cur.clear();
+          cone = bits = 0;
+          ++gen;
+        }
+      }
+      if (!cur.empty()) chunks.push_back(cur);
     }
-    if (!cur.empty()) chunks.push_back(cur);
   }
 
   // ---- 3. pack; split failures in half
@@ -183,6 +246,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
       eps.insert(eps.end(), good[i + 1].endpoints.begin(), good[i + 1].endpoints.end());
       Partition p;
       if (!build_partition(g, st, eps, p, po)) return;
+      if (opt.target_parts && p.cone_ands > cone_bound) return;  // keep the balance
       bool accept;
       if (opt.cost_model && opt.cost_model->valid()) {
         // learned rule: merge when the predicted kernel time of the merged

@@ -719,7 +719,9 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
   uint32_t pid = pid0;
   for (;;) {
     __syncthreads();
-    const long long t_start = clock64();
+    // per-partition timing (part_cycles) counts the item's own work: from
+    // its start, or from the end of the barrier wait it took over
+    long long t_start = clock64();
     if (t < 256) sh.meta[t] = __ldg(script + off + t);
     uint32_t e[16];
     {
@@ -757,6 +759,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         if (t == 0) mbar_wait(&sh.bar[0], uses0 & 1u, P.timeout);
         return;
       }
+      t_start = clock64();
     }
     // ---- global read, both lane words.  X-capable partitions of the quad
     // layout copy each slot's 16 bytes straight into shared memory with

@@ -36,6 +36,30 @@ def test_soc_like_design_with_major_stages():
     netlist_check("soc_mini", cases.script("soc_mini", 148, (20, 40, 60)), cycles=12)
 
 
+@pytest.mark.parametrize("kind,split,parts", [
+    ("soc_mini", (20, 40, 60), 5), ("small", (8, 16, 24), 3), ("sram", (8,), 2),
+])
+def test_balanced_partitions_compute_the_design(kind, split, parts):
+    """target_parts: at most `parts` partitions per major stage, the cone
+    bound taken as small as that allows, and the script still computes the
+    design."""
+    d = cases.design(kind)
+    s = d.build_script(num_blocks=16, level_split=split, merge_passes=0, target_parts=parts)
+    assert validate(s) == (0, "")
+    stage = np.asarray(s.stage_block_part)[:, 0]
+    per_stage = np.bincount(stage, minlength=s.num_major_stages)
+    assert per_stage.max() <= parts
+    ref = d.build_script(num_blocks=16, level_split=split)
+    ands, ref_ands = s.features[:, 1], ref.features[:, 1]
+    ref_stage = np.asarray(ref.stage_block_part)[:, 0]
+    for ms in range(s.num_major_stages):
+        # every stage's logic is covered; the largest partition is no larger
+        # than the default partitioner's when that one used no more of them
+        if (ref_stage == ms).sum() <= per_stage[ms]:
+            assert ands[stage == ms].max() <= ref_ands[ref_stage == ms].max()
+    netlist_check(kind, s, cycles=12)
+
+
 def validate(s, words=None, data=None, rio=None):
     from jacquard_b200.frontend import _lib
     L = _lib()
