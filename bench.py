@@ -178,10 +178,12 @@ def learned_model():
 
 def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0):
     """target_parts > 0 cuts each major stage into at most that many
-    partitions of balanced cone size, without merges: the batched kernel
-    then runs every stage as one round of work items, one per CTA (a
-    partition makes lanes / 2 lane-pair items).  Otherwise partitions come
-    from the cone target, merged by the learned rule when a model is given."""
+    partitions of balanced cone size in flat stages, without merges: the
+    batched kernel then runs every stage as one round of work items, one per
+    CTA (a partition makes lanes / 2 lane-pair items); a cost model then
+    refines the cut (endpoints move off the partition predicted slowest).
+    Otherwise partitions come from the cone target, merged by the learned
+    rule when a model is given."""
     return d.build_script(num_blocks=num_blocks, level_split=LEVEL_SPLIT, xprop=xprop,
                           target_cone=TARGET_CONE, cost_model=cost_model,
                           merge_passes=0 if target_parts else (3 if cost_model is not None else 1),
@@ -310,7 +312,7 @@ def run_mine_batched(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
-    model = None if args.no_learned else learned_model()
+    model = learned_model() if args.learned else None
     s = build_script(d, args.blocks, cost_model=model,
                      target_parts=args.blocks // max(1, args.lanes // 2))
     lanes = args.lanes
@@ -370,8 +372,9 @@ def run_mine_batched(args, rank, world):
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
-                            partitioner="balanced: at most %d per major stage"
-                            % (args.blocks // max(1, args.lanes // 2))),
+                            partitioner="balanced: at most %d per major stage%s"
+                            % (args.blocks // max(1, args.lanes // 2),
+                               ", learned refinement" if model is not None else "")),
                 script=s, d=d)
 
 
@@ -586,7 +589,8 @@ def main():
     ap.add_argument("--clusters", type=int, default=512,
                     help="design size in 4096-gate clusters (512 = the 2M-gate workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-learned", action="store_true", help="heuristic partitioner only")
+    ap.add_argument("--learned", action="store_true",
+                    help="batched: the learned cost model refines the balanced partitions")
     ap.add_argument("--compare", action="store_true",
                     help="also time the single-stream plain kernel on the same design")
     args = ap.parse_args()

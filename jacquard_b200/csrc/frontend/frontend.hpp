@@ -70,6 +70,9 @@ struct Partition {
 };
 struct PackOptions {
   int max_stages = 64;
+  // every gate at tree level 1 (one logic level per boomerang stage): the
+  // form the batched kernel evaluates as dense slot lists
+  bool flat = false;
 };
 // Builds one partition; returns false when the endpoint set does not fit the
 // 256-thread boomerang resources (the caller splits it).

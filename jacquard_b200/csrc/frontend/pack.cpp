@@ -214,8 +214,9 @@ bool build_partition(const AIG &g, const StagedAIG &st,
 
     BoomStage S;
     bool built = false;
-    // tree budget on level-1 slots; halved until phase B fits
-    int budget = 4096;
+    // tree budget on level-1 slots; halved until phase B fits (none for
+    // flat stages)
+    int budget = opt.flat ? 0 : 4096;
     for (int attempt = 0; attempt < 8 && !built; ++attempt) {
       for (int l = 0; l <= L; ++l) {
         S.hier[l].assign(lvl_len(l), NONE);

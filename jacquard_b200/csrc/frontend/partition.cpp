@@ -135,6 +135,16 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
       st.for_each_input(g, e, [&](uint32_t) { eb++; });
       return eb;
     };
+    // Balanced mode weighs an SRAM endpoint as this many AND gates: the
+    // batched kernel's SRAM port (staging, transposes, the row read and write
+    // of every stream) adds about 2.5k SM cycles to a work item, the time of
+    // about 1.2k gates at level 1.
+    constexpr uint64_t SRAM_CONE_WEIGHT = 1200;
+    const size_t nso = st.staged_outputs.size();
+    const size_t npo = g.primary_outputs.size(), nd = g.dffs.size();
+    auto weight = [&](uint32_t e) -> uint64_t {
+      return e >= nso && st.endpoints[e - nso] >= npo + nd ? SRAM_CONE_WEIGHT : 0;
+    };
     // Balanced: a chunk is closed before the endpoint whose cone would take
     // it past `bound`, so no chunk of several endpoints exceeds it.  Returns
     // the number of chunks (stored into `out` when given).
@@ -148,7 +158,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
         bool close = !cur.empty() && bits + eb > opt.target_endpoint_bits;
         uint64_t add = 0;
         if (!close) {
-          add = grow(e);
+          add = grow(e) + weight(e);
           close = !cur.empty() && cone + add > bound;
         }
         if (close) {
@@ -157,7 +167,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
           cur.clear();
           cone = bits = 0;
           ++gen;
-          add = grow(e);
+          add = grow(e) + weight(e);
         }
         cur.push_back(e);
         cone += add;
@@ -175,7 +185,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
       // chunks (binary search; the whole stage as one chunk is the top)
       uint64_t lo = 1, hi = 0;
       ++gen;
-      for (uint32_t e : order) hi += grow(e);
+      for (uint32_t e : order) hi += grow(e) + weight(e);
       hi = std::max<uint64_t>(hi, 1);
       while (lo < hi) {
         const uint64_t mid = lo + (hi - lo) / 2;
@@ -212,6 +222,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
 
   // ---- 3. pack; split failures in half
   PackOptions po;
+  po.flat = opt.target_parts != 0;  // balanced mode targets the batched kernel
   std::vector<Partition> good;
   while (!chunks.empty()) {
     std::vector<Partition> built(chunks.size());
@@ -232,6 +243,75 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
       retry.push_back(std::vector<uint32_t>(chunks[i].begin() + h, chunks[i].end()));
     }
     chunks.swap(retry);
+  }
+
+  // ---- 3b. learned refinement (balanced mode with a cost model).  All
+  // partitions of a stage run at once, so the stage lasts as long as the
+  // slowest.  While it helps, endpoints move across a boundary of the
+  // partition predicted slowest: its first or last 1/16, 1/8 or 1/4 go to
+  // the neighbour on that side, and the move that gives the smallest larger
+  // prediction of the two is taken if that is below the old maximum.
+  if (opt.target_parts && opt.cost_model && opt.cost_model->valid() && good.size() > 1) {
+    std::vector<uint32_t> pos(ne);
+    for (size_t i = 0; i < order.size(); ++i) pos[order[i]] = (uint32_t)i;
+    std::sort(good.begin(), good.end(), [&](const Partition &a, const Partition &b) {
+      return pos[a.endpoints.front()] < pos[b.endpoints.front()];
+    });
+    auto predict = [&](const Partition &p) {
+      float f[NFEAT];
+      partition_features(g, st, p, opt.xpins, f);
+      return (double)opt.cost_model->predict(f);  // log cycles
+    };
+    std::vector<double> pred(good.size());
+    parallel_for(good.size(), threads, [&](size_t i) { pred[i] = predict(good[i]); });
+    struct Move {
+      size_t j = 0, m = 0;
+      Partition a, b;  // the slowest and its neighbour after the move
+      double worse = 0;
+      bool ok = false;
+    };
+    const size_t max_steps = 4 * good.size();
+    for (size_t step = 0; step < max_steps; ++step) {
+      const size_t i = (size_t)(std::max_element(pred.begin(), pred.end()) - pred.begin());
+      const size_t n = good[i].endpoints.size();
+      std::vector<Move> moves;
+      for (size_t j : {i - 1, i + 1}) {
+        if (j >= good.size()) continue;  // i - 1 wraps for i = 0
+        for (size_t div : {16, 8, 4}) {
+          Move mv;
+          mv.j = j;
+          mv.m = std::max<size_t>(1, n / div);
+          if (mv.m < n && (moves.empty() || moves.back().j != j || moves.back().m != mv.m))
+            moves.push_back(std::move(mv));
+        }
+      }
+      parallel_for(moves.size(), threads, [&](size_t k) {
+        Move &mv = moves[k];
+        const auto &ei = good[i].endpoints, &ej = good[mv.j].endpoints;
+        std::vector<uint32_t> ni, nj;
+        if (mv.j == i + 1) {  // i's last m lead j
+          ni.assign(ei.begin(), ei.end() - mv.m);
+          nj.assign(ei.end() - mv.m, ei.end());
+          nj.insert(nj.end(), ej.begin(), ej.end());
+        } else {  // i's first m follow j
+          ni.assign(ei.begin() + mv.m, ei.end());
+          nj = ej;
+          nj.insert(nj.end(), ei.begin(), ei.begin() + mv.m);
+        }
+        if (!build_partition(g, st, ni, mv.a, po) || !build_partition(g, st, nj, mv.b, po)) return;
+        mv.worse = std::max(predict(mv.a), predict(mv.b));
+        mv.ok = true;
+      });
+      Move *best = nullptr;
+      for (auto &mv : moves)
+        if (mv.ok && (!best || mv.worse < best->worse)) best = &mv;
+      if (!best || best->worse >= pred[i] - 1e-3) break;
+      const size_t j = best->j;
+      good[i] = std::move(best->a);
+      good[j] = std::move(best->b);
+      pred[i] = predict(good[i]);
+      pred[j] = predict(good[j]);
+    }
   }
 
   // ---- 4. merge neighbours (in endpoint order) when it costs no stages

@@ -4,13 +4,17 @@
          [--out jacquard_b200/trained/costmodel.npz] [--eval-clusters 1024]
 
 1. Builds scripts of seeded SoC-family designs (the SoC workload's generator at
-   several sizes and seeds) with varied level splits and partition sizes.
-2. Runs each on the batched interpreter with per-partition timing
-   (`part_cycles`) and records log(mean SM cycles per partition work item)
+   several sizes and seeds) with varied level splits and balanced partition
+   counts per major stage.
+2. Runs each on the batched interpreter in lane-pair work items (the batched
+   workload's form) with per-partition timing (`part_cycles`, which leaves
+   out the grid-barrier wait) and records log(mean SM cycles per work item)
    next to the partition's 24 features.
 3. Trains the MLP with Adam (lr 1e-3, batch 512) on the GPU kernels.
-4. Evaluates on a fresh design: heuristic vs learned partitioner, device-timed
-   stimulus-cycles/s of the batched interpreter, same stimulus.
+4. Evaluates on a fresh design: balanced partitions without and with the
+   learned refinement (the partitioner moves endpoints off the partition
+   predicted slowest in each stage), device-timed stimulus-cycles/s of the
+   batched interpreter, same stimulus.
 """
 import argparse
 import json
@@ -20,16 +24,19 @@ import time
 import numpy as np
 import torch
 
-from . import autotune, batched, costmodel, frontend
+from . import batched, costmodel, frontend
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def measure(design, split_every, cone, lanes=4, cycles=4, blocks=148, cost_model=None):
-    s = design.build_script(num_blocks=blocks, level_split=tuple(range(split_every, 80, split_every)),
-                            xprop=True, target_cone=cone, cost_model=cost_model)
-    # single-lane items: the committed model was trained on their timings
-    B = batched.BatchedSim(s, lanes, lanes_per_item=1)
+def build(design, split_every, parts, blocks=148, cost_model=None):
+    return design.build_script(num_blocks=blocks, level_split=tuple(range(split_every, 80, split_every)),
+                               xprop=True, cost_model=cost_model, merge_passes=0, target_parts=parts)
+
+
+def measure(design, split_every, parts, lanes=8, cycles=4, blocks=148):
+    s = build(design, split_every, parts, blocks)
+    B = batched.BatchedSim(s, lanes, lanes_per_item=2)
     B.load_state(np.zeros((lanes, B.sig), np.uint32))
     B.reset_sram()
     pc = torch.zeros(s.num_partitions, dtype=torch.int64, device="cuda")
@@ -37,7 +44,7 @@ def measure(design, split_every, cone, lanes=4, cycles=4, blocks=148, cost_model
     B.run(None, cycles, part_cycles=pc)
     torch.cuda.synchronize()
     assert B.status() == 0
-    per_item = pc.cpu().numpy().astype(np.float64) / (lanes * cycles)
+    per_item = pc.cpu().numpy().astype(np.float64) / ((lanes // 2) * cycles)
     ok = per_item > 0
     return s.features[ok], np.log(per_item[ok]).astype(np.float32)
 
@@ -48,13 +55,13 @@ def collect(target, seed0=100, log=print):
     n = 0
     k = 0
     while n < target:
-        clusters = int(rng.choice([32, 64, 128]))
+        clusters = int(rng.choice([64, 128, 256]))
         d = frontend.Design(frontend.soc_params(seed=seed0 + k, n_clusters=clusters,
                                                 n_dff=200_000 * clusters // 512, n_sram=4))
-        split = int(rng.choice([4, 5, 6, 8, 10]))
-        cone = int(rng.choice([1000, 2000, 4000, 6000, 9000, 12000]))
+        split = int(rng.choice([3, 4, 5]))
+        parts = int(rng.choice([12, 18, 24, 30, 37]))
         try:
-            f, y = measure(d, split, cone)
+            f, y = measure(d, split, parts)
         except RuntimeError as e:
             log(f"  skip: {e}")
             k += 1
@@ -63,21 +70,23 @@ def collect(target, seed0=100, log=print):
         ys.append(y)
         n += len(y)
         k += 1
-        log(f"  design {k}: {clusters} clusters, split {split}, cone {cone}: {len(y)} partitions ({n} total)")
+        log(f"  design {k}: {clusters} clusters, split {split}, {parts} per stage: {len(y)} partitions ({n} total)")
     return np.concatenate(feats)[:target], np.concatenate(ys)[:target]
 
 
-def evaluate(model_packed, clusters=1024, cycles=5000, lanes=8, seed=4242, split=5, cone=6000,
+def evaluate(model_packed, clusters=1024, cycles=5000, lanes=8, seed=4242, split=4, parts=74,
              log=print):
-    """Heuristic vs learned partitioner on one fresh design: batched
-    stimulus-cycles/s over `cycles` cycles (device time, one launch each)."""
+    """Balanced partitions without and with the learned refinement on one
+    fresh design: batched stimulus-cycles/s over `cycles` cycles (device
+    time, one launch each).  74 partitions per stage make two rounds of
+    lane-pair items on 148 CTAs (37 leave partitions too large to pack)."""
     d = frontend.Design(frontend.soc_params(seed=seed, n_clusters=clusters,
                                             n_dff=200_000 * clusters // 512))
-    out = {"design_ands": int(d.num_and), "cycles": cycles, "streams": 32 * lanes}
+    out = {"design_ands": int(d.num_and), "cycles": cycles, "streams": 32 * lanes,
+           "split": split, "parts_per_stage": parts}
     for name, cm in (("heuristic", None), ("learned", model_packed)):
         t0 = time.perf_counter()
-        s = d.build_script(num_blocks=148, level_split=tuple(range(split, 80, split)), xprop=True,
-                           target_cone=cone, cost_model=cm, merge_passes=3)
+        s = build(d, split, parts, cost_model=cm)
         bt = time.perf_counter() - t0
         B = batched.BatchedSim(s, lanes)
         B.load_state(np.zeros((lanes, B.sig), np.uint32))
@@ -106,6 +115,7 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "trained", "costmodel.npz"))
     ap.add_argument("--eval-clusters", type=int, default=1024)
     ap.add_argument("--eval-cycles", type=int, default=5000)
+    ap.add_argument("--eval-parts", type=int, default=74, help="partitions per major stage")
     args = ap.parse_args()
     t0 = time.time()
     X, y = collect(args.samples)
@@ -120,10 +130,13 @@ def main():
     base = float(np.var(y[te]))
     print(f"train loss {hist[0][1]:.3f} -> {hist[-1][1]:.3f}; held-out mse {mse:.4f} (variance {base:.4f}, R^2 {1 - mse / base:.3f})")
     m.save(args.out)
-    ev = evaluate(m.pack(), clusters=args.eval_clusters, cycles=args.eval_cycles)
+    ev = evaluate(m.pack(), clusters=args.eval_clusters, cycles=args.eval_cycles,
+                  parts=args.eval_parts)
+    # the SoC workload's own design (2M gates, seed 2), one round of items
+    ev_soc = evaluate(m.pack(), clusters=512, cycles=args.eval_cycles, seed=2, parts=37)
     summary = {"samples": int(len(y)), "steps": args.steps, "loss_start": hist[0][1],
                "loss_end": hist[-1][1], "heldout_mse": mse, "heldout_var": base,
-               "heldout_r2": 1 - mse / base, "eval": ev}
+               "heldout_r2": 1 - mse / base, "eval": ev, "eval_soc2m": ev_soc}
     with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
         json.dump(summary, f, indent=1)
     print(json.dumps(summary))

@@ -25,7 +25,7 @@ def design(kind, seed=11):
 
 
 @functools.lru_cache(maxsize=None)
-def script(kind, num_blocks, split=(), xprop=False, timing_seed=0):
+def script(kind, num_blocks, split=(), xprop=False, timing_seed=0, target_parts=0):
     d = design(kind)
     if timing_seed:
         rng = np.random.default_rng(timing_seed)
@@ -34,7 +34,11 @@ def script(kind, num_blocks, split=(), xprop=False, timing_seed=0):
         r = rng.integers(20, 201, size=n).astype(np.uint32)
         r[kinds != 1] = 0
         d.set_delays(r, r)
-    s = d.build_script(num_blocks=num_blocks, level_split=split, xprop=xprop)
+    if target_parts:  # balanced, flat partitions (the batched workload's form)
+        s = d.build_script(num_blocks=num_blocks, level_split=split, xprop=xprop,
+                           merge_passes=0, target_parts=target_parts)
+    else:
+        s = d.build_script(num_blocks=num_blocks, level_split=split, xprop=xprop)
     if timing_seed:
         d.set_delays(np.zeros(d.num_pins + 1, np.uint32), np.zeros(d.num_pins + 1, np.uint32))
     return s

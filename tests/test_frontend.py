@@ -60,6 +60,22 @@ def test_balanced_partitions_compute_the_design(kind, split, parts):
     netlist_check(kind, s, cycles=12)
 
 
+def test_learned_refinement_keeps_the_design():
+    """With a cost model the balanced partitioner moves endpoints between
+    neighbouring partitions; every endpoint stays computed."""
+    import os
+    from jacquard_b200 import costmodel
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "jacquard_b200", "trained", "costmodel.npz")
+    d = cases.design("soc_mini")
+    s = d.build_script(num_blocks=16, level_split=(20, 40, 60), merge_passes=0,
+                       target_parts=5, cost_model=costmodel.packed_from_file(path))
+    assert validate(s) == (0, "")
+    assert np.bincount(np.asarray(s.stage_block_part)[:, 0]).max() <= 5
+    assert int(s.features[:, 14].max()) <= 1
+    netlist_check("soc_mini", s, cycles=12)
+
+
 def validate(s, words=None, data=None, rio=None):
     from jacquard_b200.frontend import _lib
     L = _lib()

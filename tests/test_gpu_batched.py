@@ -32,7 +32,24 @@ def per_stream_states(kind, s, cycles, streams, x_init):
 ])
 def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slots, per_item,
                                            grid):
-    s = cases.script(kind, nb, split, xprop=xprop)
+    check_batched(kind, cases.script(kind, nb, split, xprop=xprop), lanes, wo_slots, per_item, grid)
+
+
+@pytest.mark.parametrize("kind,nb,split,parts,lanes,grid", [
+    ("soc_mini", 148, (20, 40, 60), 37, 2, 0),   # one item per CTA per stage
+    ("soc_mini", 148, (20, 40, 60), 37, 2, 5),   # tickets
+    ("sram", 16, (8,), 4, 2, 0),
+])
+def test_batched_balanced_partitions_match_oracle(kind, nb, split, parts, lanes, grid):
+    """Balanced, flat partitions (every gate at tree level 1, the batched
+    workload's script form) in lane-pair items."""
+    s = cases.script(kind, nb, split, xprop=True, target_parts=parts)
+    assert int(s.features[:, 14].max()) <= 1  # deepest tree level with a gate
+    check_batched(kind, s, lanes, None, 2, grid)
+
+
+def check_batched(kind, s, lanes, wo_slots, per_item, grid):
+    xprop = s.xprop_enabled
     cycles = 10
     S = 32 * lanes
     snaps = per_stream_states(kind, s, cycles, S, x_init=xprop)
