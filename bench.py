@@ -46,7 +46,7 @@ WORKLOADS = {
 # workload: dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
 # jq_batched_kernel (a 4-cycle launch after 3 warm-up launches), divided by
 # its 4 cycles; traffic grows in proportion to the cycle count.
-BATCHED_DRAM_BYTES_PER_CYCLE = (531.187968e6 + 264.023552e6) / 4
+BATCHED_DRAM_BYTES_PER_CYCLE = (567.099136e6 + 270.249984e6) / 4
 
 
 def peaks():
