@@ -1,13 +1,13 @@
 """Autotuner for the batched interpreter on one design: sweeps the level
-split granularity, the partitioner's cone target (partition size), the number
-of script blocks and the cycles per launch, timing each configuration on the
-device with CUDA events, and returns the fastest.
+split granularity, the partition size (the partitioner's cone target, or its
+balanced mode with one round of lane-pair work items per major stage), the
+number of script blocks and the cycles per launch, timing each configuration
+on the device with CUDA events, and returns the fastest.
 
 Each configuration is a full script build (host) plus a short timed run; the
 result records the stimulus-cycles/s of every point so the choice is
 reproducible.
 """
-import itertools
 import time
 
 import numpy as np
@@ -16,12 +16,21 @@ import torch
 from . import batched
 
 
+def balanced_parts(blocks, lanes):
+    """Partitions per major stage for one round of lane-pair items: each
+    partition makes lanes / 2 items, one per CTA."""
+    return max(1, blocks // max(1, lanes // 2))
+
+
 def time_config(design, split_every, cone, blocks, window, lanes, cost_model=None, reps=2,
-                device="cuda"):
+                device="cuda", parts=0):
+    """cone: the partitioner's cone target; parts > 0 selects balanced mode
+    (at most `parts` partitions per major stage, no merges) instead."""
     depth_split = tuple(range(split_every, 80, split_every))
     t0 = time.perf_counter()
     s = design.build_script(num_blocks=blocks, level_split=depth_split, xprop=True,
-                            target_cone=cone, cost_model=cost_model)
+                            target_cone=cone, cost_model=cost_model,
+                            merge_passes=0 if parts else 1, target_parts=parts)
     build_s = time.perf_counter() - t0
     B = batched.BatchedSim(s, lanes, device=device)
     B.load_state(np.zeros((lanes, B.sig), np.uint32))
@@ -39,16 +48,21 @@ def time_config(design, split_every, cone, blocks, window, lanes, cost_model=Non
     assert B.status() == 0
     ms = e0.elapsed_time(e1) / reps
     rate = 32 * lanes * window / (ms / 1e3)
-    return dict(split_every=split_every, cone=cone, blocks=blocks, window=window, lanes=lanes,
+    return dict(split_every=split_every, cone=cone, parts=parts, blocks=blocks, window=window,
+                lanes=lanes,
                 stream_cycles_per_s=rate, us_per_cycle=ms * 1e3 / window,
                 partitions=s.num_partitions, script_mb=s.script_words_per_cycle() * 4 / 1e6,
                 build_s=build_s)
 
 
-def sweep(design, splits=(5, 8, 10), cones=(512, 2000, 6000, 8000), blocks=(148, 296, 592),
-          windows=(1, 16, 64, 256), lanes=8, budget_s=600.0, log=print):
-    """Coarse-to-fine: (split, cone) at the default blocks/window, then blocks
-    and window around the best point.  Stops when budget_s is spent."""
+def sweep(design, splits=(3, 4, 5, 8, 10), cones=(512, 2000, 6000, 8000),
+          blocks=(148, 296, 592), windows=(1, 16, 64, 256), lanes=8, budget_s=600.0, log=print,
+          timer=None):
+    """Coarse-to-fine: (split, partition size) at the default blocks/window,
+    then blocks and window around the best point.  Partition sizes are the
+    cone targets plus balanced mode (cone 0 in the results).  Stops when
+    budget_s is spent.  `timer` replaces time_config (same keywords)."""
+    timer = timer or time_config
     t_start = time.perf_counter()
     results = []
 
@@ -56,24 +70,33 @@ def sweep(design, splits=(5, 8, 10), cones=(512, 2000, 6000, 8000), blocks=(148,
         if time.perf_counter() - t_start > budget_s:
             return None
         try:
-            r = time_config(design, lanes=lanes, **kw)
+            r = timer(design, lanes=lanes, **kw)
         except RuntimeError as e:  # a partition that cannot be packed
             log(f"  skip {kw}: {e}")
             return None
         results.append(r)
-        log(f"  {r['split_every']:>2} {r['cone']:>5} {r['blocks']:>4} {r['window']:>4}: "
+        size = f"{r['parts']}/st" if r["parts"] else str(r["cone"])
+        log(f"  {r['split_every']:>2} {size:>6} {r['blocks']:>4} {r['window']:>4}: "
             f"{r['stream_cycles_per_s']:>12.0f} stream-cycles/s  ({r['partitions']} parts, "
             f"{r['script_mb']:.1f} MB script, build {r['build_s']:.1f}s)")
         return r
 
-    for sp, cone in itertools.product(splits, cones):
-        run(split_every=sp, cone=cone, blocks=blocks[0], window=16)
+    for sp in splits:
+        for cone in cones:
+            run(split_every=sp, cone=cone, blocks=blocks[0], window=16)
+        run(split_every=sp, cone=0, blocks=blocks[0], window=16,
+            parts=balanced_parts(blocks[0], lanes))
     best = max(results, key=lambda r: r["stream_cycles_per_s"])
+
+    def size_of(r, nb):  # the best point's partition size at nb blocks
+        return dict(cone=r["cone"], parts=balanced_parts(nb, lanes) if r["parts"] else 0)
+
     for nb in blocks[1:]:
-        run(split_every=best["split_every"], cone=best["cone"], blocks=nb, window=16)
+        run(split_every=best["split_every"], blocks=nb, window=16, **size_of(best, nb))
     best = max(results, key=lambda r: r["stream_cycles_per_s"])
     for w in windows:
         if w != 16:
-            run(split_every=best["split_every"], cone=best["cone"], blocks=best["blocks"], window=w)
+            run(split_every=best["split_every"], blocks=best["blocks"], window=w,
+                cone=best["cone"], parts=best["parts"])
     best = max(results, key=lambda r: r["stream_cycles_per_s"])
     return best, results
