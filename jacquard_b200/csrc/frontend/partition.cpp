@@ -14,6 +14,10 @@
 //      retried (the reference's halving loop, src/sim/setup.rs:540-580);
 //   4. neighbouring small partitions are merged when the merged one still
 //      packs without more stages (src/pe.rs:855-1070's acceptance rule).
+// Balanced mode (target_parts) replaces step 2 with the smallest cone bound
+// that cuts the stage into at most target_parts chunks, packs flat stages,
+// and, given a cost model, refines the cut (step 3b) before merging within
+// the bound.
 #include "frontend.hpp"
 
 #include <algorithm>
