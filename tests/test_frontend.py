@@ -60,6 +60,22 @@ def test_balanced_partitions_compute_the_design(kind, split, parts):
     netlist_check(kind, s, cycles=12)
 
 
+@pytest.mark.parametrize("parts", [1, 1000])
+def test_balanced_partition_count_extremes(parts):
+    """One partition per stage, and more allowed partitions than endpoints
+    (the bound falls to single endpoints' cones)."""
+    d = cases.design("tiny")
+    s = d.build_script(num_blocks=4, level_split=(5,), merge_passes=0, target_parts=parts)
+    assert validate(s) == (0, "")
+    per_stage = np.bincount(np.asarray(s.stage_block_part)[:, 0], minlength=s.num_major_stages)
+    assert per_stage.max() <= parts
+    if parts == 1:
+        assert (per_stage == 1).all()
+    else:
+        assert s.features[:, 1].max() <= 32  # one endpoint's cone (4-5 levels)
+    netlist_check("tiny", s, cycles=12)
+
+
 def test_learned_refinement_keeps_the_design():
     """With a cost model the balanced partitioner moves endpoints between
     neighbouring partitions; every endpoint stays computed."""
