@@ -178,3 +178,22 @@ def test_windowed_timed_run_drains_every_violation():
     want_multiset = sorted((int(r[2]), "setup" if r[0] == 4 else "hold", int(r[4]), timing._s32(r[5]))
                            for r in np.concatenate(want_ev))
     assert got_multiset == want_multiset
+
+
+def test_barrier_wait_that_runs_out_is_reported():
+    """A grid-barrier wait limited to one SM cycle runs out for every CTA
+    that arrives before the last: the launch ends with
+    JQ_ERR_BARRIER_TIMEOUT (every CTA returns at its next barrier at the
+    latest), and the next launch on the same context runs normally."""
+    s = cases.script("tiny", 148, (5,))
+    states = cases.stimulus("tiny", s, 8)
+    ds = sim.DeviceScript(s)
+    st = sim.u32_to_dev(states.reshape(-1))
+    n_sram = max(1, s.sram_storage_size)
+    sram = sim.u32_to_dev(np.zeros(n_sram, np.uint32))
+    sram_x = sim.u32_to_dev(np.full(n_sram, 0xFFFFFFFF, np.uint32))
+    sim.simulate(ds, st, 8, states.shape[1], sram, sram_x, barrier_timeout_cycles=1)
+    assert sim.status() == -3  # JQ_ERR_BARRIER_TIMEOUT
+    want, _, _, _ = run_oracle(s, states, 8)
+    got, _, _, _ = run_gpu(s, states, 8)  # checks status 0 itself
+    assert np.array_equal(got, want)
