@@ -1,0 +1,53 @@
+"""The committed, trained partition cost model on the host (no GPU): its
+training summary records the learned-vs-heuristic comparison, and it
+predicts the cost structure the simulator measured."""
+import json
+import os
+
+import numpy as np
+
+from jacquard_b200 import costmodel, frontend
+
+TRAINED = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "jacquard_b200", "trained")
+
+
+def predict(model, feats):
+    feats = np.ascontiguousarray(feats, np.float32)
+    out = np.zeros(len(feats), np.float32)
+    L = frontend._lib()
+    r = L.jqf_cost_model_predict(model.ctypes.data, feats.ctypes.data, len(feats), out.ctypes.data)
+    assert r == 0
+    return out
+
+
+def test_summary_records_learned_vs_heuristic():
+    with open(os.path.join(TRAINED, "costmodel.json")) as f:
+        sm = json.load(f)
+    assert sm["samples"] >= 20000 and sm["steps"] == 2000
+    assert sm["heldout_r2"] > 0.9
+    for key in ("eval", "eval_soc2m"):
+        ev = sm[key]
+        h, l = ev["heuristic"]["stream_cycles_per_s"], ev["learned"]["stream_cycles_per_s"]
+        assert h > 0 and l > 0
+        assert abs(ev["gain"] - l / h) < 1e-9
+        assert ev["cycles"] == 5000 and ev["streams"] == 256
+
+
+def test_model_predicts_larger_partitions_cost_more():
+    """A fresh design of the training family (SoC generator, 64 clusters,
+    level split every 4) cut into 12 and into 37 balanced partitions per
+    stage: the larger partitions are predicted to take longer, as measured,
+    and within the coarse cut prediction grows with gate count."""
+    model = costmodel.packed_from_file(os.path.join(TRAINED, "costmodel.npz"))
+    d = frontend.Design(frontend.soc_params(seed=77, n_clusters=64, n_dff=200_000 * 64 // 512,
+                                            n_sram=4))
+    split = tuple(range(4, 80, 4))
+    big = d.build_script(num_blocks=148, level_split=split, xprop=True, merge_passes=0,
+                         target_parts=12)
+    small = d.build_script(num_blocks=148, level_split=split, xprop=True, merge_passes=0,
+                           target_parts=37)
+    assert big.features[:, 1].mean() > 2 * small.features[:, 1].mean()
+    pb, ps = predict(model, big.features), predict(model, small.features)
+    assert np.exp(pb).mean() > np.exp(ps).mean()
+    assert np.corrcoef(big.features[:, 1], pb)[0, 1] > 0.3
