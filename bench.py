@@ -4,9 +4,12 @@ single-port 1024x32 SRAMs, 128 PIs, X-propagation on, all DFF/SRAM state X at
 start, 16 reset cycles then p_toggle = 0.25 stimulus).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
-                  [--mode plain|batched] [--lanes L] [--window C]
+                  [--mode plain|batched] [--lanes L] [--window C] [--learned]
 
-One step = one launch window of C cycles over all stimulus streams.  `value`
+One step = one launch window of C cycles over all stimulus streams.  The
+batched mode partitions every major stage into blocks / (lanes / 2) balanced
+partitions (one round of lane-pair work items); --learned adds the cost
+model's refinement of that cut.  `value`
 is device-timed throughput with inputs resident in HBM; `e2e` is the same
 through the C ABI with host buffers copied in and out inside the timed region.
 --impl reference runs the reference's CPU interpreter path (this repository's
