@@ -45,11 +45,28 @@ WORKLOADS = {
 }
 
 
-# DRAM bytes (read + write) per simulated cycle of the 256-stream batched
-# workload: dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
-# jq_batched_kernel (a 4-cycle launch after 3 warm-up launches), divided by
-# its 4 cycles; traffic grows in proportion to the cycle count.
-BATCHED_DRAM_BYTES_PER_CYCLE = (567.099136e6 + 270.249984e6) / 4
+PROFILE_BATCHED = os.path.join(HERE, "profiles", "batched_kernel_soc2M_xprop.md")
+KERNEL_SRC = os.path.join(HERE, "jacquard_b200", "csrc", "sim_batched.cu")
+
+
+def measured_traffic_per_cycle():
+    """DRAM bytes (read + write) per simulated cycle of the 256-stream batched
+    workload, from the ncu capture summarised in the kernel's profile (a
+    line `traffic_bytes_per_cycle: B source_sha256: H`), or None when that
+    capture was taken of another version of the kernel source."""
+    import hashlib
+    import re
+    try:
+        with open(PROFILE_BATCHED) as f:
+            m = re.search(r"traffic_bytes_per_cycle:\s*([0-9.eE+]+)\s+source_sha256:\s*([0-9a-f]+)",
+                          f.read())
+        with open(KERNEL_SRC, "rb") as f:
+            h = hashlib.sha256(f.read()).hexdigest()
+    except OSError:
+        return None
+    if not m or not h.startswith(m.group(2)):
+        return None
+    return float(m.group(1))
 
 
 def peaks():
@@ -193,14 +210,23 @@ def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0):
                           target_parts=target_parts)
 
 
-def algorithmic_bytes_per_cycle(s, lanes=1, arrivals=False):
-    """Bytes one simulated cycle must move (per the boomerang format): script
-    words (counted once per launch pass over `lanes` lane groups), non-empty
-    global-read words, IO read-old + write, SRAM read/read/write, each with
-    its X-mask copy on X-capable partitions; state terms scale with lanes."""
+def algorithmic_bytes_per_cycle(s, streams=1, arrivals=False, bit_sliced=False):
+    """(script bytes, state bytes) one simulated cycle must move.
+
+    Script: every word of the script (FlattenedScriptV1, empty-block dummies
+    included), read once per cycle however many streams share it.
+    State, per partition (x = 1 on X-capable partitions): the global-read
+    bits, the IO words read (old value) and written, the SRAM words (read,
+    old word at the write address, write), each with its X copy.
+    Plain layout (one stream): a 4-byte state word per non-empty global-read
+    word and per IO word, 3 words per SRAM.  Bit-sliced layout (`streams`
+    streams, a lane word holding one signal of 32 streams): a lane word per
+    selected global-read bit and per IO signal, per 32 streams; SRAM words
+    stay per stream."""
     bd = s.blocks_data
     script_words = int(s.blocks_start[-1])
     gr = io = sr = 0
+    lane_words = (streams + 31) // 32
     for b in range(s.num_blocks * s.num_major_stages):
         off = int(s.blocks_start[b])
         while True:
@@ -210,14 +236,20 @@ def algorithmic_bytes_per_cycle(s, lanes=1, arrivals=False):
             nio, R, nsr, isx = int(bd[off + 2]), int(bd[off + 6]), int(bd[off + 4]), int(bd[off + 8])
             m = bd[off + 256: off + 256 + 512 * R].reshape(-1, 2)[:, 1]
             k = 1 + (1 if isx else 0)
-            gr += int(np.count_nonzero(m)) * k
-            io += 2 * nio * k + (nio if arrivals else 0)
-            sr += 3 * nsr * k
+            if bit_sliced:
+                bits = int(np.unpackbits(np.ascontiguousarray(m).view(np.uint8)).sum())
+                gr += bits * k * lane_words
+                io += (2 * k + (1 if arrivals else 0)) * nio * 32 * lane_words
+                sr += 3 * nsr * k * streams
+            else:
+                gr += int(np.count_nonzero(m)) * k * streams
+                io += (2 * nio * k + (nio if arrivals else 0)) * streams
+                sr += 3 * nsr * k * streams
             last = int(bd[off + 1])
             off += 256 + 512 * R + 5120 * (ns + 2)
             if last:
                 break
-    return 4 * script_words, 4 * (gr + io + sr) * lanes
+    return 4 * script_words, 4 * (gr + io + sr)
 
 
 def stimulus_window(s, d, first_cycle, cycles, seed):
@@ -289,7 +321,8 @@ def run_mine_plain(args, rank, world):
     e2e_ms = e0.elapsed_time(e1)
     script_b, state_b = algorithmic_bytes_per_cycle(s)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=1, clocks=ck.summary(),
-                bytes_per_cycle=script_b + state_b, kernel_ms=dev_ms / args.steps,
+                bytes_per_cycle=script_b + state_b, script_bytes=script_b,
+                kernel_ms=dev_ms / args.steps,
                 h2d=host_pin.numel() * 4, d2h=out_pin.numel() * 4, launches_per_step=2,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
@@ -307,6 +340,76 @@ def batched_stimulus(s, d, streams, cycles, seed0, first=0):
         vals = state.stimulus_inputs(s, d, first + cycles, seed0 + k, P_TOGGLE, RESET_CYCLES)
         per[k] = state.pack_inputs(s, vals[first:first + cycles + 1])[:, :words]
     return batched.to_batched(per)
+
+
+class StreamCheck:
+    """Bit-exactness self-check of timed batched windows: stream k is
+    replayed on the plain interpreter (this library's single-stream kernel,
+    the reference's state layout) from the batched state where a timed
+    region started, over the same windows, and must end in the same state
+    and SRAM contents and record the same outputs in the last window.
+    Runs outside the timed regions."""
+
+    def __init__(self, B, s, d, stim, streams):
+        import torch
+        from jacquard_b200 import sim
+        self.B, self.s, self.stim, self.streams = B, s, stim, streams
+        self.ds = sim.DeviceScript(s, B.device)
+        self.eff = B.sig // 32
+        self.words = B.in_sigs // 32
+
+    def _stream(self, lane_major, k):
+        """Words (eff,) of stream k from a lane-major (lanes, sig) device tensor."""
+        import torch
+        lane, bit = divmod(k, 32)
+        b = ((lane_major[lane] >> bit) & 1).to(torch.int64).view(-1, 32)
+        return ((b << torch.arange(32, device=b.device)).sum(-1) & 0xFFFFFFFF).to(torch.int64)
+
+    def capture(self):
+        """The batched state and SRAM of the checked streams, now."""
+        import torch
+        B = self.B
+        cur = B.final_state(0).view(B.lanes, B.sig)  # state_a: every window is even
+        sram = B.sram.view(32 * B.lanes, -1)
+        sram_x = B.sram_x.view(32 * B.lanes, -1)
+        return {k: (self._stream(cur, k), sram[k].clone(), sram_x[k].clone()) for k in self.streams}
+
+    def replay(self, start, end, windows, wave):
+        """True when every checked stream, replayed `windows` windows from
+        `start`, reaches `end` with the same outputs in the last window."""
+        import torch
+        from jacquard_b200 import sim
+        B, W = self.B, self.stim.shape[0] - 1
+        eff, words = self.eff, self.words
+        npo = B.n_po
+        ok = True
+        for k in self.streams:
+            lane, bit = divmod(k, 32)
+            st0, sram, sram_x = (t.clone() for t in start[k])
+            inp = torch.from_numpy(np.ascontiguousarray(
+                (self.stim[:, lane, :] >> np.uint32(bit)) & 1).astype(np.int64)).to(B.device)
+            inp = (inp.view(W + 1, words, 32) << torch.arange(32, device=B.device)).sum(-1)
+            snaps = torch.empty((W + 1, eff), dtype=torch.int64, device=B.device)
+            cur = st0.to(torch.int64)
+            sram, sram_x = sram.to(torch.int32), sram_x.to(torch.int32)
+            for _ in range(windows):
+                snaps[:] = cur
+                snaps[1:, :words] = inp[1:]
+                buf = (snaps - ((snaps >> 31) << 32)).to(torch.int32)  # u32 bits as int32
+                sim.simulate(self.ds, buf, W, eff, sram, sram_x)
+                if sim.status() != 0:
+                    return False
+                cur = buf[W].to(torch.int64) & 0xFFFFFFFF
+            e_st, e_sram, e_sx = end[k]
+            ok &= bool(torch.equal(cur, e_st)) and bool(torch.equal(sram, e_sram)) \
+                and bool(torch.equal(sram_x, e_sx))
+            if npo:
+                po = B.po.to(torch.int64)
+                last = (buf[1:].to(torch.int64) & 0xFFFFFFFF).index_select(1, po >> 5)
+                want = (last >> (po & 31)) & 1
+                got = ((wave.view(W, npo, B.lanes)[:, :, lane] >> bit) & 1).to(torch.int64)
+                ok &= bool(torch.equal(got, want))
+        return ok
 
 
 def run_mine_batched(args, rank, world):
@@ -340,10 +443,12 @@ def run_mine_batched(args, rank, world):
     wave = torch.empty(W * len(po_sig) * lanes, dtype=torch.int32, device=dev)
     wave_pin = torch.empty(wave.numel(), dtype=torch.int32).pin_memory()
     stream = torch.cuda.current_stream(dev)
+    check = StreamCheck(B, s, d, stim, (0, streams - 1)) if not args.no_check else None
     for _ in range(args.warmup):
         B.run(stim_dev, W, wave=wave, stream=stream)
     torch.cuda.synchronize()
     assert B.status(stream) == 0
+    at_start = check.capture() if check else None
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     with Clocks(dev.index) as ck:
@@ -355,6 +460,8 @@ def run_mine_batched(args, rank, world):
         timed_region_edge(world)
     dev_ms = t0.elapsed_time(t1)
     assert B.status(stream) == 0
+    at_mid = check.capture() if check else None
+    wave_dev_region = wave.clone() if check else None
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     timed_region_edge(world)
@@ -367,11 +474,17 @@ def run_mine_batched(args, rank, world):
     timed_region_edge(world)
     e2e_ms = e0.elapsed_time(e1)
     assert B.status(stream) == 0
-    script_b, state_b = algorithmic_bytes_per_cycle(s)
+    parity = None
+    if check:
+        at_end = check.capture()
+        parity = (check.replay(at_start, at_mid, args.steps, wave_dev_region)
+                  and check.replay(at_mid, at_end, args.steps, wave_pin.to(dev)))
+    script_b, state_b = algorithmic_bytes_per_cycle(s, streams=streams, bit_sliced=True)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams,
-                clocks=ck.summary(), bytes_per_cycle=script_b + state_b * streams,
+                clocks=ck.summary(), bytes_per_cycle=script_b + state_b, script_bytes=script_b,
                 kernel_ms=dev_ms / args.steps, h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4,
-                launches_per_step=2,
+                launches_per_step=2, parity=parity,
+                traffic_per_cycle=measured_traffic_per_cycle() if args.clusters == 512 else None,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
@@ -456,7 +569,8 @@ def run_mine_timed(args, rank, world):
     e2e_ms = e0.elapsed_time(e1)
     script_b, state_b = algorithmic_bytes_per_cycle(s, arrivals=True)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=1, clocks=ck.summary(),
-                bytes_per_cycle=script_b + state_b, kernel_ms=dev_ms / args.steps,
+                bytes_per_cycle=script_b + state_b, script_bytes=script_b,
+                kernel_ms=dev_ms / args.steps,
                 h2d=(W + 1) * eff * 4, d2h=W * eff * 4, launches_per_step=2,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=rio,
@@ -520,10 +634,11 @@ def run_mine_multi(args, rank, world):
     dev_ms = t0.elapsed_time(t1)
     assert B.status(stream) == 0
     streams = 32 * lanes * len(scripts)
-    per = [algorithmic_bytes_per_cycle(s) for s in scripts]
-    bytes_per_cycle = sum(p[0] for p in per) + 32 * lanes * sum(p[1] for p in per)
+    per = [algorithmic_bytes_per_cycle(s, streams=32 * lanes, bit_sliced=True) for s in scripts]
+    bytes_per_cycle = sum(p[0] + p[1] for p in per)
     return dict(dev_ms=dev_ms, e2e_ms=None, cycles_per_step=W, streams=streams,
-                clocks=ck.summary(), bytes_per_cycle=bytes_per_cycle, kernel_ms=dev_ms / args.steps,
+                clocks=ck.summary(), bytes_per_cycle=bytes_per_cycle,
+                script_bytes=sum(p[0] for p in per), kernel_ms=dev_ms / args.steps,
                 h2d=0, d2h=0, launches_per_step=2,
                 design=dict(designs=len(scripts), ands=ands, sizes=sizes.tolist(),
                             partitions=int(sum(s.num_partitions for s in scripts)),
@@ -594,6 +709,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--learned", action="store_true",
                     help="batched: the learned cost model refines the balanced partitions")
+    ap.add_argument("--no-check", action="store_true",
+                    help="batched: skip the bit-exactness self-check of the timed windows")
     ap.add_argument("--compare", action="store_true",
                     help="also time the single-stream plain kernel on the same design")
     args = ap.parse_args()
@@ -648,7 +765,10 @@ def main():
         dist.barrier()
     if rank == 0:
         peak, peak_kind = peaks()
-        achieved = r["bytes_per_cycle"] * r["cycles_per_step"] / (r["kernel_ms"] / 1e3) / 1e9
+        cyc_per_s = r["cycles_per_step"] / (r["kernel_ms"] / 1e3)
+        achieved = r["bytes_per_cycle"] * cyc_per_s / 1e9
+        script_gbs = r["script_bytes"] * cyc_per_s / 1e9
+        tpc = r.get("traffic_per_cycle")
         if args.no_cpu or args.mode in ("timed", "multi"):
             cpu_v, cpu_dt = None, 0.0
         else:
@@ -665,8 +785,9 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
                              "algorithmic_bytes_per_launch": r["bytes_per_cycle"] * r["cycles_per_step"],
-                             "traffic": (BATCHED_DRAM_BYTES_PER_CYCLE * r["cycles_per_step"]
-                                         if args.mode == "batched" and args.clusters == 512 else None)},
+                             "script_gbs": script_gbs, "script_frac": script_gbs / peak,
+                             "traffic": tpc * r["cycles_per_step"] if tpc else None,
+                             "traffic_frac": (tpc * cyc_per_s / 1e9 / peak) if tpc else None},
                 "cpu_baseline": {"value": cpu_v, "unit": "stimulus-cycles/s", "cores": 1,
                                  "kind": "port",
                                  "sample": f"{args.cpu_cycles} cycles x 1 stream, {cpu_dt:.1f} s"},
@@ -675,6 +796,8 @@ def main():
                         if e2e_val is not None else None),
                 "gpu_launches": r["launches_per_step"] * args.steps,
                 "clocks": r["clocks"]}
+        if r.get("parity") is not None:
+            line["parity"] = r["parity"]
         if args.compare and args.mode == "batched":
             line["compare"] = compare_kernels(r["d"], args)
         print(json.dumps(line))

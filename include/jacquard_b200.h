@@ -8,9 +8,15 @@
  * calls from sim_cuda (src/bin/jacquard.rs:1135-1147):
  *   simulate_v1_noninteractive_simple_scan_cuda  <- csrc/kernel_v1.cu:17-46
  *   simulate_v1_noninteractive_timed_cuda        <- csrc/kernel_v1.cu:49-78
- * All pointers are caller-owned DEVICE pointers; the launch is asynchronous
- * on the legacy default stream; like the reference, a launch failure prints
- * the CUDA error and exits the process (csrc/kernel_v1.cu:6-14).
+ * All pointers are caller-owned DEVICE pointers; the launch runs on the
+ * legacy default stream.  Like the reference, a launch failure prints the
+ * CUDA error and exits the process (csrc/kernel_v1.cu:6-14).  Unlike the
+ * reference's grid.sync(), this interpreter's grid barrier has a bounded
+ * wait; a launch that ran out of it has left the snapshots half-written, so
+ * the wrappers wait for the launch, and print and exit on that error too.
+ * They therefore return with the work done (the reference returns right
+ * after the launch; its caller synchronizes next, src/bin/jacquard.rs:1131,
+ * 1149).
  *
  * The jq_* entry points below have no counterpart symbol in the reference:
  * they return a status instead of exiting, take an explicit stream, report
@@ -64,6 +70,7 @@ void simulate_v1_noninteractive_timed_cuda(
 #define JQ_ERR_CUDA -4            /* asynchronous CUDA error */
 #define JQ_ERR_TOO_MANY_BLOCKS -5 /* grid larger than co-resident capacity */
 #define JQ_ERR_NOALLOC_LIMIT -6   /* request exceeds a fixed built-in workspace */
+#define JQ_ERR_TOO_MANY_STREAMS -7 /* launches on more streams than barrier slots */
 #define JQ_ERR_EVENT_OVERFLOW 1   /* positive: events were dropped */
 
 /* Event record: identical to the reference's Event (32 bytes). */
@@ -96,13 +103,25 @@ typedef struct {
   void *stream; /* cudaStream_t, NULL = legacy default stream */
 } jq_sim_args;
 
+/* Barrier slots.  Each interpreter (plain, batched) keeps its grid-barrier
+ * counters and its error status in module memory, 64 slots per device.  A
+ * launch takes the slot of the (device, stream) it is issued on: launches on
+ * one stream share it and run in stream order, launches on different streams
+ * get different slots, so they may overlap on the GPU.  Slots are never
+ * released; the 65th distinct stream of a process gets
+ * JQ_ERR_TOO_MANY_STREAMS.  NULL and cudaStreamLegacy are one stream;
+ * cudaStreamPerThread is one handle for all host threads, so launches on it
+ * from several threads must not overlap.  A launch captured in a CUDA graph
+ * keeps the slot of the stream it was captured on. */
+
 /* Plain interpreter (reference layout, one stimulus stream).  Asynchronous;
  * returns JQ_OK or a launch error.  Kernel-side status (barrier timeout) is
- * read back with jq_sim_status. */
+ * read back with jq_sim_status on the same stream. */
 int jq_simulate(const jq_sim_args *a);
 
 /* Synchronizes `stream` and returns JQ_OK, JQ_ERR_BARRIER_TIMEOUT or
- * JQ_ERR_CUDA for the launches made so far on it, and clears the flag. */
+ * JQ_ERR_CUDA for the plain launches made so far on it, and clears the
+ * recorded error. */
 int jq_sim_status(void *stream);
 
 /* Largest grid the plain interpreter can keep co-resident on `device`. */
@@ -208,7 +227,8 @@ int jq_batched_pack_state(const uint32_t *lane_major, uint32_t lanes, size_t sig
                           int32_t x_interleaved, uint32_t *state, void *stream);
 int jq_batched_unpack_state(const uint32_t *state, uint32_t lanes, size_t signals,
                             int32_t x_interleaved, uint32_t *lane_major, void *stream);
-/* Synchronizes `stream`; JQ_OK or the kernel's recorded error. */
+/* Synchronizes `stream`; JQ_OK or the recorded error of the batched launches
+ * made on it (cleared by the read).  Barrier slots as for jq_simulate. */
 int jq_batched_status(void *stream);
 int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks);
 int jq_batched_smem_bytes(uint32_t wo_slots);
@@ -257,13 +277,17 @@ int jq_mlp_train_step(const jq_mlp_step_args *a);
 /* No counterpart in the reference.  Same as jq_mlp_train_step but allocates
  * nothing and ignores a->scratch: the per-CTA gradient workspace is a
  * file-scope device array of JQ_MLP_NOALLOC_MAX_CTAS rows (about 1.3 MB, held
- * on every GPU that loads the library until exit).  For callers that cannot
- * call cudaMalloc, e.g. while a CUDA graph is being captured or under a fixed
- * pre-sized device pool.  a->scratch_ctas must be 1..JQ_MLP_NOALLOC_MAX_CTAS,
- * otherwise JQ_ERR_NOALLOC_LIMIT.  The first call on a device resolves the
- * array's address and should come before any stream capture.  All calls on
- * a device share the array: calls that overlap on the GPU race.  Nothing in
- * it needs clearing; each call writes every entry it reads. */
+ * on every GPU that loads the library until exit).  For hosts that cannot
+ * allocate device memory once running: an embedding host with one device
+ * pool sized at start-up, or one whose latency limits rule out an allocation
+ * that may synchronize the device.  a->scratch_ctas must be
+ * 1..JQ_MLP_NOALLOC_MAX_CTAS, otherwise JQ_ERR_NOALLOC_LIMIT; a NULL `a` is
+ * JQ_ERR_INVALID_ARG.  Every call resolves the array's address for the
+ * current device and context (cudaGetSymbolAddress, which allocates
+ * nothing); the first call on a device may also load the library's module
+ * there, so make it before any stream capture.  All calls on a device share
+ * the array: calls that overlap on the GPU race.  Nothing in it needs
+ * clearing; each call writes every entry it reads. */
 #define JQ_MLP_NOALLOC_MAX_CTAS 16
 int jq_mlp_train_step_noalloc(const jq_mlp_step_args *a);
 

@@ -241,8 +241,11 @@ class BatchedSim:
             base[k] = nxt
         return base
 
-    def run(self, stim, cycles, wave=None, record_buf=None, stream=None, part_cycles=None):
-        """stim: device tensor [(cycles+1) * lanes * in_sigs] int32 or None."""
+    def run(self, stim, cycles, wave=None, record_buf=None, stream=None, part_cycles=None,
+            barrier_timeout_cycles=0):
+        """stim: device tensor [(cycles+1) * lanes * in_sigs] int32 or None.
+        barrier_timeout_cycles: grid-barrier wait limit in SM clocks (0 = the
+        library's default of about a second)."""
         L = lib()
         wave_ptr = wave.data_ptr() if wave is not None else None
         a = BatchArgs(self.ds.num_blocks, self.ds.num_major_stages, self.ds.blocks_start.data_ptr(),
@@ -257,7 +260,7 @@ class BatchedSim:
                       self.wo_slots, self.block_list.data_ptr(), self.block_list_start.data_ptr(),
                       part_cycles.data_ptr() if part_cycles is not None else None,
                       self.part_base_dev.data_ptr(), self.gr_sources.data_ptr(),
-                      self.grid, 0,
+                      self.grid, barrier_timeout_cycles,
                       stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream,
                       self.lanes_per_item, self.x_interleaved)
         rc = L.jq_simulate_batched(ctypes.byref(a))

@@ -271,31 +271,29 @@ int jq_mlp_train_step(const jq_mlp_step_args *a) {
 // ------------------------------------------------------------------------
 // No-allocation variant of jq_mlp_train_step.
 //
-// Some callers cannot call cudaMalloc (or any allocating routine) at the
-// point where they train: a host that issues its work while a CUDA graph is
-// being captured, or an embedding host that owns a fixed, pre-sized device
-// pool and forbids allocation at run time.  For them the gradient workspace
-// lives in this file-scope device array instead of a caller buffer.  It holds
-// JQ_MLP_NOALLOC_MAX_CTAS partial-gradient rows (about 1.3 MB) on every GPU
-// that loads the library, until the process exits.
+// Some hosts cannot call cudaMalloc (or any routine that allocates) once they
+// are running: an embedding host that sizes one device pool at start-up and
+// forbids allocation afterwards, or a host with hard latency limits where an
+// allocation may stall on a device-wide synchronization.  For them the
+// gradient workspace lives in this file-scope device array instead of a
+// caller buffer.  It holds JQ_MLP_NOALLOC_MAX_CTAS partial-gradient rows
+// (about 1.3 MB) on every GPU that loads the library, until the process
+// exits.
 static __device__ __align__(256) float g_mlp_noalloc_scratch[JQ_MLP_NOALLOC_MAX_CTAS * (JQ_MLP_PARAMS + 1)];
-static float *g_mlp_noalloc_ptr[64];  // device address of the array, per device
 
 int jq_mlp_train_step_noalloc(const jq_mlp_step_args *a) {
-  if (!a || a->scratch_ctas == 0 || a->scratch_ctas > JQ_MLP_NOALLOC_MAX_CTAS)
+  if (!a) return JQ_ERR_INVALID_ARG;
+  if (a->scratch_ctas == 0 || a->scratch_ctas > JQ_MLP_NOALLOC_MAX_CTAS)
     return JQ_ERR_NOALLOC_LIMIT;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return JQ_ERR_CUDA;
-  if (!g_mlp_noalloc_ptr[dev]) {
-    // First call on this device: resolve the array's device address with the
-    // device current.  The host-side symbol is only a stand-in and must never
-    // be handed to a kernel.
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_mlp_noalloc_scratch) != cudaSuccess || !p) return JQ_ERR_CUDA;
-    g_mlp_noalloc_ptr[dev] = static_cast<float *>(p);
-  }
+  // The array's device address, for the current device and context.  The
+  // host-side symbol is only a stand-in and must never be handed to a kernel.
+  // It is resolved on every call (this allocates nothing) rather than cached,
+  // because the module's address changes when the context does (another
+  // context made current by the host, or a device reset).
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_mlp_noalloc_scratch) != cudaSuccess || !p) return JQ_ERR_CUDA;
   jq_mlp_step_args b = *a;
-  b.scratch = g_mlp_noalloc_ptr[dev];
+  b.scratch = static_cast<float *>(p);
   return jq_mlp_train_step(&b);
 }
 

@@ -76,7 +76,9 @@ struct BatchParams {
   const uint32_t *part_base;         // first partition index of (stage, block)
   const uint32_t *gr_sources;        // per partition: source signal of each of
                                      // the 8192 global-read positions
-  uint64_t timeout;
+  uint64_t timeout;        // grid-barrier wait limit (SM clocks)
+  uint64_t chunk_timeout;  // script-chunk copy wait limit: fixed, so a short
+                           // barrier limit never leaves a copy in flight
   int slot;
 };
 
@@ -385,14 +387,15 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
       }
       uint32_t &uses = b ? uses1 : uses0;
       // warp-uniform, so the shuffles below run with full warps
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.timeout));
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.chunk_timeout));
       ++uses;
       // a chunk never arrived: every thread leaves together, after letting
       // the copy still in flight into the other buffer land
 #define JQ_FAIL_IF(cond)                                               \
   if (__syncthreads_or(cond)) {                                        \
     failed = true;                                                     \
-    if (t == 0) mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.timeout); \
+    if (t == 0 && ci + 1 < nchunks)                                    \
+      mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.chunk_timeout);  \
     return;                                                            \
   }
       // hooks of a compact stage: 32-slot blocks of its region
@@ -756,7 +759,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
             for (uint32_t l = i0; l < nl; l += n) prefetch_l2(rows + 32 * (size_t)l);
           })) {
         failed = true;
-        if (t == 0) mbar_wait(&sh.bar[0], uses0 & 1u, P.timeout);
+        if (t == 0) mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout);
         return;
       }
       t_start = clock64();
@@ -834,12 +837,13 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
                     &sh.bar[b ^ 1]);
       }
       uint32_t &uses = b ? uses1 : uses0;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.timeout));
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.chunk_timeout));
       ++uses;
 #define JQ_FAIL_IF(cond)                                               \
   if (__syncthreads_or(cond)) {                                        \
     failed = true;                                                     \
-    if (t == 0) mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.timeout); \
+    if (t == 0 && ci + 1 < nchunks)                                    \
+      mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.chunk_timeout);  \
     return;                                                            \
   }
 #define JQ_HOOKS_COMPACT(stage, pbase)                                                        \
@@ -1951,7 +1955,9 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.gr_sources = a->gr_sources;
   if (!P.part_base || !P.gr_sources) return JQ_ERR_INVALID_ARG;
   P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
-  P.slot = 1;
+  P.chunk_timeout = DEFAULT_BARRIER_TIMEOUT;
+  P.slot = launch_slot(a->stream, true);
+  if (P.slot < 0) return JQ_ERR_TOO_MANY_STREAMS;
   jq_batched_reset_kernel<<<1, 1, 0, st>>>(P.slot);
   if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
   const int smem = (int)smem_layout_bytes(P.wo_slots, v);
@@ -1962,12 +1968,15 @@ int jq_simulate_batched(const jq_batch_args *a) {
 
 int jq_batched_status(void *stream) {
   if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return JQ_ERR_CUDA;
-  int flags[1] = {0};
-  if (cudaMemcpyFromSymbol(flags, g_status, sizeof(int), 1 * sizeof(int)) != cudaSuccess)
+  const int slot = launch_slot(stream, false);
+  if (slot < 0) return JQ_OK;  // nothing launched on this stream
+  int flag = 0;
+  if (cudaMemcpyFromSymbol(&flag, g_status, sizeof(int), slot * sizeof(int)) != cudaSuccess)
     return JQ_ERR_CUDA;
-  static const int zero_i[1] = {0};
-  cudaMemcpyToSymbol(g_status, zero_i, sizeof(int), 1 * sizeof(int));
-  return flags[0];
+  static const int zero = 0;
+  if (cudaMemcpyToSymbol(g_status, &zero, sizeof(int), slot * sizeof(int)) != cudaSuccess)
+    return JQ_ERR_CUDA;
+  return flag;
 }
 
 }  // extern "C"

@@ -15,11 +15,17 @@ constexpr uint64_t DEFAULT_BARRIER_TIMEOUT = 2000000000ull;  // ~1 s at 2 GHz
 
 // Grid barrier state lives in module memory (no allocation on the call path);
 // each translation unit that includes this header has its own copy.  One slot
-// per concurrently running launch; launches on one slot must not overlap.
-// g_bar_count returns to 0 after every completed barrier.
+// per stream a launch is issued on (launch_slot); launches on one slot run in
+// stream order and never overlap.  g_bar_count returns to 0 after every
+// completed barrier.
 static __device__ unsigned int g_bar_count[BAR_SLOTS];
 static __device__ unsigned int g_bar_gen[BAR_SLOTS];
 static __device__ int g_status[BAR_SLOTS];
+
+// Slot of the (current device, stream) pair (launch_slots.cu): assigns a free
+// one when `assign` and the pair has none yet; -1 when the table is full or,
+// without `assign`, when nothing was launched on the pair.
+int launch_slot(void *stream, bool assign);
 
 __device__ __forceinline__ uint4 ldg4(const uint32_t *p) {
   return __ldg(reinterpret_cast<const uint4 *>(p));

@@ -304,12 +304,14 @@ __global__ void jq_plain_reset_kernel(int slot) {
 
 int g_max_blocks_cache[64];
 
-int launch_plain(const jq_sim_args *a, uint32_t event_cap, int slot) {
+int launch_plain(const jq_sim_args *a, uint32_t event_cap) {
   if (!a || a->num_blocks == 0 || a->num_major_stages == 0 || a->num_major_stages > 32 ||
       !a->blocks_start || !a->blocks_data || !a->states)
     return JQ_ERR_INVALID_ARG;
   if (a->timing_constraints && !a->events) return JQ_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)a->stream;
+  const int slot = launch_slot(a->stream, true);
+  if (slot < 0) return JQ_ERR_TOO_MANY_STREAMS;
   const bool track = a->arrival_state_offset != 0 || a->timing_constraints != nullptr;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -351,6 +353,37 @@ void die_on(int rc, const char *what) {
   exit(EXIT_FAILURE);
 }
 
+// Status of the slot's launches so far: JQ_OK, the kernel's recorded error,
+// or JQ_ERR_CUDA.  Synchronizes the stream and clears the recorded error.
+int read_status(void *stream) {
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return JQ_ERR_CUDA;
+  const int slot = launch_slot(stream, false);
+  if (slot < 0) return JQ_OK;  // nothing launched on this stream
+  int flag = 0;
+  if (cudaMemcpyFromSymbol(&flag, g_status, sizeof(int), slot * sizeof(int)) != cudaSuccess)
+    return JQ_ERR_CUDA;
+  static const int zero = 0;
+  if (cudaMemcpyToSymbol(g_status, &zero, sizeof(int), slot * sizeof(int)) != cudaSuccess)
+    return JQ_ERR_CUDA;
+  return flag;
+}
+
+// The legacy wrappers: launch on the legacy default stream, then wait for
+// the launch and exit on any error, as the reference's checkCudaErrors does
+// for launch errors (csrc/kernel_v1.cu:6-14).  The reference's grid.sync()
+// cannot time out; this interpreter's bounded barrier can, and a launch that
+// ended that way has left the snapshots half-written, so it is an error here
+// too.  The wait makes these calls synchronous; their caller synchronizes
+// right after them anyway (src/bin/jacquard.rs:1131, 1149).
+void legacy_launch(const jq_sim_args *a, uint32_t event_cap, const char *what) {
+  die_on(launch_plain(a, event_cap), what);
+  const int rc = read_status(nullptr);
+  if (rc == JQ_OK) return;
+  printf("CUDA error at %s: %s (%s)\n", what, jq_strerror(rc),
+         cudaGetErrorString(cudaGetLastError()));
+  exit(EXIT_FAILURE);
+}
+
 }  // namespace
 
 extern "C" {
@@ -370,19 +403,9 @@ int jq_max_blocks(int device, size_t *max_blocks) {
   return JQ_OK;
 }
 
-int jq_simulate(const jq_sim_args *a) {
-  return launch_plain(a, a ? a->event_capacity : 0, 0);
-}
+int jq_simulate(const jq_sim_args *a) { return launch_plain(a, a ? a->event_capacity : 0); }
 
-int jq_sim_status(void *stream) {
-  cudaStream_t st = (cudaStream_t)stream;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return JQ_ERR_CUDA;
-  int flags[1] = {0};
-  if (cudaMemcpyFromSymbol(flags, g_status, sizeof(int), 0) != cudaSuccess) return JQ_ERR_CUDA;
-  static const int zero_i[1] = {0};
-  cudaMemcpyToSymbol(g_status, zero_i, sizeof(int), 0);
-  return flags[0];
-}
+int jq_sim_status(void *stream) { return read_status(stream); }
 
 const char *jq_strerror(int code) {
   switch (code) {
@@ -393,6 +416,8 @@ const char *jq_strerror(int code) {
     case JQ_ERR_CUDA: return "CUDA error";
     case JQ_ERR_TOO_MANY_BLOCKS: return "more blocks than can be co-resident";
     case JQ_ERR_EVENT_OVERFLOW: return "event buffer overflowed";
+    case JQ_ERR_TOO_MANY_STREAMS:
+      return "launches on more distinct streams than the interpreter has barrier slots";
     case JQ_ERR_NOALLOC_LIMIT:
       return "request exceeds the built-in no-allocation workspace (JQ_MLP_NOALLOC_MAX_CTAS CTAs)";
     default: return "unknown status";
@@ -416,7 +441,7 @@ void simulate_v1_noninteractive_simple_scan_cuda(size_t num_blocks, size_t num_m
   a.state_size = state_size;
   a.states = states_noninteractive;
   a.arrival_state_offset = arrival_state_offset;
-  die_on(launch_plain(&a, 0, 0), "simulate_v1_noninteractive_simple_scan_cuda");
+  legacy_launch(&a, 0, "simulate_v1_noninteractive_simple_scan_cuda");
 }
 
 void simulate_v1_noninteractive_timed_cuda(size_t num_blocks, size_t num_major_stages,
@@ -440,7 +465,7 @@ void simulate_v1_noninteractive_timed_cuda(size_t num_blocks, size_t num_major_s
   a.events = (jq_event_buffer *)event_buffer;
   a.arrival_state_offset = arrival_state_offset;
   // the reference's EventBuffer holds MAX_EVENTS = 1024 records
-  die_on(launch_plain(&a, 1024, 0), "simulate_v1_noninteractive_timed_cuda");
+  legacy_launch(&a, 1024, "simulate_v1_noninteractive_timed_cuda");
 }
 
 }  // extern "C"

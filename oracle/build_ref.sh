@@ -7,8 +7,10 @@
 # (-maxrregcount=128, -lineinfo) plus the sm_100a target.
 # Output is test infrastructure: the reference arm of the parity tests and the
 # reference-GPU timing line.  Nothing in the product links it.
+# The reference tree: the first argument, else JQ_REFERENCE_ROOT, else the
+# location this container mounts it at.
 set -euo pipefail
-REF=${JQ_REFERENCE_ROOT:-/root/reference}
+REF=${1:-${JQ_REFERENCE_ROOT:-/root/reference}}
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/csrc/kernel_v1.cu" ]; then

@@ -48,40 +48,96 @@ def test_batched_balanced_partitions_match_oracle(kind, nb, split, parts, lanes,
     check_batched(kind, s, lanes, None, 2, grid)
 
 
+class BatchedCase:
+    """A batched run prepared on the device with its per-stream oracle
+    results: launch() issues it (on any stream), verify() checks every
+    snapshot and SRAM word of every stream."""
+
+    def __init__(self, kind, s, lanes, wo_slots=None, per_item=0, grid=0, cycles=10, seed0=1000):
+        xprop = s.xprop_enabled
+        self.cycles, self.lanes, self.S = cycles, lanes, 32 * lanes
+        snaps = np.stack([cases.stimulus(kind, s, cycles, seed=seed0 + k, x_init=xprop)
+                          for k in range(self.S)])  # (S, cycles+1, eff)
+        self.eff = snaps.shape[-1]
+        self.want = snaps.copy()
+        self.wsram = []
+        for k in range(self.S):  # oracle, stream by stream
+            st = self.want[k].reshape(-1).copy()
+            sram = np.zeros(max(1, s.sram_storage_size), np.uint32)
+            sram_x = np.full_like(sram, 0xFFFFFFFF)
+            oracle_lib.simulate(s, st, cycles, self.eff, sram=sram, sram_x=sram_x)
+            self.want[k] = st.reshape(cycles + 1, self.eff)
+            self.wsram.append(sram)
+        self.B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots,
+                                    lanes_per_item=per_item, grid=grid)
+        self.bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
+        B = self.B
+        self.stim = torch.from_numpy(
+            np.ascontiguousarray(self.bt[:, :, :B.in_sigs]).reshape(-1).view(np.int32)).cuda()
+        self.rec = torch.zeros((cycles + 1) * B.sig * lanes, dtype=torch.int32, device="cuda")
+        self.reset()
+
+    def reset(self):
+        B = self.B
+        B.load_state(self.bt[0])
+        B.reset_sram()
+        self.rec.zero_()
+        self.rec[: B.sig * self.lanes].copy_(
+            torch.from_numpy(np.ascontiguousarray(self.bt[0]).reshape(-1).view(np.int32)))
+
+    def launch(self, stream=None, barrier_timeout_cycles=0):
+        self.B.run(self.stim, self.cycles, record_buf=self.rec, stream=stream,
+                   barrier_timeout_cycles=barrier_timeout_cycles)
+
+    def verify(self):
+        B = self.B
+        got = batched.from_batched(
+            self.rec.cpu().numpy().view(np.uint32).reshape(self.cycles + 1, self.lanes, B.sig), self.eff)
+        assert got.shape == self.want.shape
+        for k in range(self.S):
+            assert np.array_equal(got[k], self.want[k]), f"stream {k}"
+        gs = B.sram.cpu().numpy().view(np.uint32).reshape(self.S, -1)
+        for k in range(self.S):
+            assert np.array_equal(gs[k][: self.wsram[k].size], self.wsram[k])
+
+
 def check_batched(kind, s, lanes, wo_slots, per_item, grid):
-    xprop = s.xprop_enabled
-    cycles = 10
-    S = 32 * lanes
-    snaps = per_stream_states(kind, s, cycles, S, x_init=xprop)
-    eff = snaps.shape[-1]
-    # oracle, stream by stream
-    want = snaps.copy()
-    wsram = []
-    for k in range(S):
-        st = want[k].reshape(-1).copy()
-        sram = np.zeros(max(1, s.sram_storage_size), np.uint32)
-        sram_x = np.full_like(sram, 0xFFFFFFFF)
-        oracle_lib.simulate(s, st, cycles, eff, sram=sram, sram_x=sram_x)
-        want[k] = st.reshape(cycles + 1, eff)
-        wsram.append(sram)
-    # batched
-    B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots, lanes_per_item=per_item,
-                           grid=grid)
-    bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
-    B.load_state(bt[0])
-    B.reset_sram()
-    stim = torch.from_numpy(np.ascontiguousarray(bt[:, :, :B.in_sigs]).reshape(-1).view(np.int32)).cuda()
-    rec = torch.zeros((cycles + 1) * B.sig * lanes, dtype=torch.int32, device="cuda")
-    rec[: B.sig * lanes].copy_(torch.from_numpy(np.ascontiguousarray(bt[0]).reshape(-1).view(np.int32)))
-    B.run(stim, cycles, record_buf=rec)
-    assert B.status() == 0
-    got = batched.from_batched(rec.cpu().numpy().view(np.uint32).reshape(cycles + 1, lanes, B.sig), eff)
-    assert got.shape == want.shape
-    for k in range(S):
-        assert np.array_equal(got[k], want[k]), f"stream {k}"
-    gs = B.sram.cpu().numpy().view(np.uint32).reshape(S, -1)
-    for k in range(S):
-        assert np.array_equal(gs[k][: wsram[k].size], wsram[k])
+    c = BatchedCase(kind, s, lanes, wo_slots, per_item, grid)
+    c.launch()
+    assert c.B.status() == 0
+    c.verify()
+
+
+def test_batched_launches_on_two_streams_overlap_safely():
+    """Two batched launches on different streams, each on a few CTAs so both
+    are resident at once: each takes its own barrier/ticket/status slot, and
+    both match the oracle stream by stream."""
+    a = BatchedCase("soc_mini", cases.script("soc_mini", 148, (20, 40, 60), xprop=True,
+                                             target_parts=37), 2, per_item=2, grid=5)
+    b = BatchedCase("sram", cases.script("sram", 16, (8,), xprop=True), 2, per_item=2, grid=4,
+                    seed0=3000)
+    torch.cuda.synchronize()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    a.launch(stream=s1)
+    b.launch(stream=s2)
+    assert a.B.status(s1) == 0 and b.B.status(s2) == 0
+    a.verify()
+    b.verify()
+
+
+def test_batched_barrier_wait_that_runs_out_is_reported():
+    """A grid-barrier wait limited to one SM clock runs out: the launch ends
+    with JQ_ERR_BARRIER_TIMEOUT (script-chunk copies keep their own fixed
+    limit, so no CTA leaves with a copy in flight), and a normal launch
+    afterwards on the same context matches the oracle."""
+    c = BatchedCase("soc_mini", cases.script("soc_mini", 148, (20, 40, 60), xprop=True,
+                                             target_parts=37), 2, per_item=2)
+    c.launch(barrier_timeout_cycles=1)
+    assert c.B.status() == -3  # JQ_ERR_BARRIER_TIMEOUT
+    c.reset()
+    c.launch()
+    assert c.B.status() == 0
+    c.verify()
 
 
 def test_lane_pairs_rejected_for_odd_lanes():

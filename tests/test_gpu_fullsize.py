@@ -58,16 +58,18 @@ def stream_of(rec, k):
     return (bits << torch.arange(32, device=rec.device)).sum(-1)
 
 
-def test_batched_256_streams_match_plain_and_oracle(soc):
-    d, s = soc
+def check_256_streams(d, s, packed, cycles, po_sig=None):
+    """The batched interpreter over 256 streams (per-stream packed inputs
+    `packed[k]`, (cycles+1, rio)) against the plain interpreter stream by
+    stream: every snapshot (values and X) and the SRAM contents of every
+    stream, the recorded outputs when `po_sig` is given; the first and last
+    streams also against the oracle."""
     rio = s.reg_io_state_size
     eff = 2 * rio
     streams = 32 * LANES
     tmpl = state.xmask_template(s)
     x0 = state.xmask_all_state_x(s)
-    packed = [stream_inputs(s, d, k, CYCLES) for k in range(streams)]
-
-    B = batched.BatchedSim(s, LANES, record=True)
+    B = batched.BatchedSim(s, LANES, record=True, po_signals=po_sig)
     words = batched.input_words(s)
     stim = batched.to_batched(np.stack([p[:, :words] for p in packed]))  # (C+1, lanes, in_sigs)
     snap0 = np.zeros((LANES, B.sig), np.uint32)
@@ -77,26 +79,33 @@ def test_batched_256_streams_match_plain_and_oracle(soc):
     B.load_state(snap0)
     B.reset_sram(x=True)
     dstim = torch.from_numpy(np.ascontiguousarray(stim).reshape(-1).view(np.int32)).cuda()
-    rec = torch.zeros((CYCLES + 1, LANES, B.sig), dtype=torch.int32, device="cuda")
+    rec = torch.zeros((cycles + 1, LANES, B.sig), dtype=torch.int32, device="cuda")
     rec[0].copy_(torch.from_numpy(snap0.view(np.int32)))
-    B.run(dstim, CYCLES, record_buf=rec)
+    wave = None
+    if po_sig is not None:
+        wave = torch.zeros(cycles * len(po_sig) * LANES, dtype=torch.int32, device="cuda")
+    B.run(dstim, cycles, record_buf=rec, wave=wave)
     assert B.status() == 0
     bsram = B.sram.view(streams, -1)
     bsram_x = B.sram_x.view(streams, -1)
+    if wave is not None:  # recorded outputs = the output signals of each snapshot
+        w = wave.view(cycles, len(po_sig), LANES)
+        po = torch.tensor(np.asarray(po_sig, np.int64), device="cuda")
+        assert torch.equal(w, rec[1:].index_select(2, po).transpose(1, 2))
 
     ds = sim.DeviceScript(s)
     n_sram = max(1, s.sram_storage_size)
     mask = torch.tensor(0xFFFFFFFF, dtype=torch.int64, device="cuda")
-    oracle_streams = {0: None, streams - 1: None}
+    oracle_streams = {0, streams - 1}
     for k in range(streams):
         host = stream_snapshots(s, packed[k], tmpl, x0)
         st = sim.u32_to_dev(host.reshape(-1))
         sram = torch.zeros(n_sram, dtype=torch.int32, device="cuda")
         sram_x = torch.full((n_sram,), -1, dtype=torch.int32, device="cuda")
-        sim.simulate(ds, st, CYCLES, eff, sram, sram_x)
+        sim.simulate(ds, st, cycles, eff, sram, sram_x)
         assert sim.status() == 0
         got = stream_of(rec, k)
-        want = st.view(CYCLES + 1, eff).to(torch.int64) & mask
+        want = st.view(cycles + 1, eff).to(torch.int64) & mask
         assert torch.equal(got, want), f"stream {k}: batched != plain"
         assert torch.equal(bsram[k, :n_sram], sram), f"stream {k}: SRAM"
         assert torch.equal(bsram_x[k, :n_sram], sram_x), f"stream {k}: SRAM X"
@@ -104,13 +113,39 @@ def test_batched_256_streams_match_plain_and_oracle(soc):
             ost = host.reshape(-1).copy()
             osram = np.zeros(n_sram, np.uint32)
             osram_x = np.full(n_sram, 0xFFFFFFFF, np.uint32)
-            oracle_lib.simulate(s, ost, CYCLES, eff, sram=osram, sram_x=osram_x, threads=THREADS)
+            oracle_lib.simulate(s, ost, cycles, eff, sram=osram, sram_x=osram_x, threads=THREADS)
             assert np.array_equal(sim.dev_to_u32(st), ost), f"stream {k}: plain != oracle"
             assert np.array_equal(sim.dev_to_u32(sram), osram)
             assert np.array_equal(sim.dev_to_u32(sram_x), osram_x)
     # the run did real work: DFF values known after reset and changing afterwards
-    last = sim.dev_to_u32(st).reshape(CYCLES + 1, eff)
+    last = sim.dev_to_u32(st).reshape(cycles + 1, eff)
     assert np.count_nonzero(last[-1, :rio] != last[-2, :rio]) > 0
+
+
+def test_batched_256_streams_match_plain_and_oracle(soc):
+    d, s = soc
+    packed = [stream_inputs(s, d, k, CYCLES) for k in range(32 * LANES)]
+    check_256_streams(d, s, packed, CYCLES)
+
+
+def test_benchmark_script_and_stimulus_256_streams_64_cycles():
+    """The exact configuration bench.py times: its design, its script
+    (148 blocks, balanced partitions, at most 37 per major stage, flat stages
+    in the compact form), its stimulus (16 reset cycles, then p_toggle 0.25,
+    stream k seeded 1000 + k) and one of its 64-cycle windows with the
+    output waveform, 256 streams: every snapshot of every stream against the
+    plain interpreter, two streams against the oracle."""
+    import bench
+    d = bench.build_design()
+    s = bench.build_script(d, 148, target_parts=37)
+    assert s.num_partitions == 740
+    assert int(s.features[:, 14].max()) <= 1  # flat stages: the compact form
+    cycles = 64
+    packed = []
+    for k in range(32 * LANES):
+        vals = state.stimulus_inputs(s, d, cycles, 1000 + k, bench.P_TOGGLE, bench.RESET_CYCLES)
+        packed.append(state.pack_inputs(s, vals))
+    check_256_streams(d, s, packed, cycles, po_sig=state.po_positions(s, d))
 
 
 def test_timed_path_full_size_matches_oracle(soc):

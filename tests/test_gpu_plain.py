@@ -135,6 +135,96 @@ def test_reference_kernel_matches_oracle(xprop):
     assert np.array_equal(sim.dev_to_u32(sram)[:wsram.size], wsram)
 
 
+def run_ref(s, states, cycles, constraints=None, arrival_off=0):
+    """The reference's own kernel through its own wrappers: the untimed one,
+    or with constraints the timed one with its 1024-slot EventBuffer
+    (csrc/event_buffer.h:45-50, zeroed).  Returns snapshots, SRAM, SRAM X
+    and (events, count, overflow) when timed."""
+    L = ctypes.CDLL(REF_SO)
+    sz, vp = ctypes.c_size_t, ctypes.c_void_p
+    L.simulate_v1_noninteractive_simple_scan_cuda.argtypes = [sz, sz, vp, vp, vp, vp, sz, sz, vp,
+                                                              ctypes.c_int32]
+    L.simulate_v1_noninteractive_timed_cuda.argtypes = [sz, sz, vp, vp, vp, vp, sz, sz, vp, vp, vp,
+                                                        ctypes.c_int32]
+    ds = sim.DeviceScript(s)
+    st = sim.u32_to_dev(states.reshape(-1))
+    n_sram = max(1, s.sram_storage_size)
+    sram = torch.zeros(n_sram, dtype=torch.int32, device="cuda")
+    sram_x = torch.full((n_sram,), -1, dtype=torch.int32, device="cuda")
+    common = (s.num_blocks, s.num_major_stages, ds.blocks_start.data_ptr(), ds.blocks_data.data_ptr(),
+              sram.data_ptr(), sram_x.data_ptr(), cycles, states.shape[1], st.data_ptr())
+    evs = None
+    if constraints is None:
+        L.simulate_v1_noninteractive_simple_scan_cuda(*common, arrival_off)
+    else:
+        cons = sim.u32_to_dev(constraints)
+        eb = torch.zeros(4 + 1024 * 8, dtype=torch.int32, device="cuda")
+        L.simulate_v1_noninteractive_timed_cuda(*common, cons.data_ptr(), eb.data_ptr(), arrival_off)
+    torch.cuda.synchronize()
+    if constraints is not None:
+        h = sim.dev_to_u32(eb[:4])
+        n = min(int(h[0]), 1024)
+        evs = (sim.dev_to_u32(eb[4:4 + 8 * n]).reshape(n, 8), int(h[0]), int(h[1]))
+    return (sim.dev_to_u32(st).reshape(states.shape), sim.dev_to_u32(sram), sim.dev_to_u32(sram_x),
+            evs)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference kernel not built")
+@pytest.mark.parametrize("xprop", [False, True])
+def test_reference_kernel_arrivals_match_oracle_and_plain(xprop):
+    """Arrivals pinned to the reference itself: its kernel writes the u16
+    arrival of every committed word when arrival_state_offset != 0
+    (csrc/kernel_v1_impl.cuh:529-533).  On a script with per-pin delays,
+    the reference kernel, the oracle and this plain interpreter give the
+    same snapshots word for word, arrival section included."""
+    s = cases.script("sram", 16, (8,), xprop=xprop, timing_seed=9)
+    s.enable_timing_arrivals()
+    try:
+        states = cases.stimulus("sram", s, 24, x_init=xprop)
+        off = s.arrival_state_offset
+        want, wsram, _, _ = run_oracle(s, states, 24, arrival_off=off)
+        ref, rsram, _, _ = run_ref(s, states, 24, arrival_off=off)
+        got, gsram, _, _ = run_gpu(s, states, 24, arrival_off=off)
+    finally:
+        s.timing_arrivals_enabled = False
+        s.arrival_state_offset = 0
+    arr = ref[1:, off:off + s.reg_io_state_size]
+    assert np.count_nonzero(arr) > 0  # the delays produced arrivals
+    assert np.array_equal(ref, want)
+    assert np.array_equal(got, want)
+    assert np.array_equal(rsram[:wsram.size], wsram) and np.array_equal(gsram[:wsram.size], wsram)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference kernel not built")
+def test_reference_timed_wrapper_events_match_oracle_and_plain():
+    """Setup/hold events pinned to the reference itself: its timed wrapper
+    (csrc/kernel_v1.cu:49-78) with a zeroed 1024-slot EventBuffer, on a case
+    that yields 624 events (setup and hold), against the oracle and this
+    library's legacy timed symbol: the same snapshots and the same sorted
+    event multiset (the order is that of atomicAdd)."""
+    s = cases.script("sram", 16, (8,), timing_seed=9)
+    s.enable_timing_arrivals()
+    try:
+        states = cases.stimulus("sram", s, 24)
+        off = s.arrival_state_offset
+        cons = cases.constraint_buffer("sram", s, clock_ps=120, setup=30, hold=150)
+        want, _, _, (wev, wcnt) = run_oracle(s, states, 24, constraints=cons, cap=1024,
+                                             arrival_off=off)
+        ref, _, _, (rev, rcnt, rov) = run_ref(s, states, 24, constraints=cons, arrival_off=off)
+        got, _, _, (gev, gcnt, gov) = run_gpu(s, states, 24, constraints=cons, cap=1024,
+                                              arrival_off=off, legacy=True)
+    finally:
+        s.timing_arrivals_enabled = False
+        s.arrival_state_offset = 0
+    assert 0 < wcnt < 1024 and rov == 0 and gov == 0
+    assert rcnt == wcnt and gcnt == wcnt
+    w = wev.view(np.uint32).reshape(-1, 8)
+    assert set(w[:, 0].tolist()) == {4, 5}  # both setup and hold violations
+    assert sorted_events(rev) == sorted_events(w)
+    assert sorted_events(gev) == sorted_events(w)
+    assert np.array_equal(ref, want) and np.array_equal(got, want)
+
+
 def test_windowed_timed_run_drains_every_violation():
     """Timed path over several launch windows with per-window event drains
     (the CUDA timed path the reference never wired) vs the oracle run with
@@ -197,3 +287,28 @@ def test_barrier_wait_that_runs_out_is_reported():
     want, _, _, _ = run_oracle(s, states, 8)
     got, _, _, _ = run_gpu(s, states, 8)  # checks status 0 itself
     assert np.array_equal(got, want)
+
+
+def test_launches_on_two_streams_overlap_safely():
+    """Two plain launches on different streams of one device, issued back to
+    back so they overlap: each takes its own barrier/status slot, and both
+    match the oracle."""
+    runs = []
+    for kind, nb, split in (("tiny", 4, ()), ("sram", 16, (8,))):
+        s = cases.script(kind, nb, split)
+        states = cases.stimulus(kind, s, 40, seed=21)
+        want, wsram, _, _ = run_oracle(s, states, 40)
+        ds = sim.DeviceScript(s)
+        st = sim.u32_to_dev(states.reshape(-1))
+        n_sram = max(1, s.sram_storage_size)
+        sram = sim.u32_to_dev(np.zeros(n_sram, np.uint32))
+        sram_x = sim.u32_to_dev(np.full(n_sram, 0xFFFFFFFF, np.uint32))
+        runs.append((ds, st, states.shape, sram, sram_x, want, wsram))
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for (ds, st, shape, sram, sram_x, _, _), stream in zip(runs, streams):
+        sim.simulate(ds, st, 40, shape[1], sram, sram_x, stream=stream)
+    for (ds, st, shape, sram, _, want, wsram), stream in zip(runs, streams):
+        assert sim.status(stream) == 0
+        assert np.array_equal(sim.dev_to_u32(st).reshape(shape), want)
+        assert np.array_equal(sim.dev_to_u32(sram)[:wsram.size], wsram)

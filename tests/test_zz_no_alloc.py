@@ -1,10 +1,11 @@
 """The no-allocation training step (jq_mlp_train_step_noalloc) against the
 regular one (jq_mlp_train_step), called through the C ABI.
 
-The no-allocation entry point is for callers that cannot call cudaMalloc --
-code issuing work while a CUDA graph is being captured, or a host with a fixed
-pre-sized device pool -- so its gradient workspace is a built-in device array
-instead of a caller buffer.  Kept in its own file, collected last."""
+The no-allocation entry point is for hosts that cannot allocate device memory
+once running -- an embedding host with one device pool sized at start-up, or
+one whose latency limits rule out an allocation that may synchronize the
+device -- so its gradient workspace is a built-in device array instead of a
+caller buffer.  Kept in its own file, collected last."""
 import ctypes
 import os
 
@@ -83,8 +84,42 @@ def test_noalloc_step_matches_regular_step_twice():
         assert close(noalloc[2], regular[2]) and close(noalloc[3], regular[3])
 
 
-def test_noalloc_rejects_oversized_request():
+def test_noalloc_limit_and_no_device_allocation():
+    """16 CTAs (the built-in array's capacity) run and match the regular step
+    with free device memory unchanged across the call; 17 are refused with
+    JQ_ERR_NOALLOC_LIMIT and a NULL argument block with JQ_ERR_INVALID_ARG."""
     L = lib()
-    a = StepArgs()
-    a.scratch_ctas = 17
-    assert L.jq_mlp_train_step_noalloc(ctypes.byref(a)) == -6
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(11)
+    n, batch, ctas = 700, 384, 16
+    X = torch.from_numpy(rng.normal(size=(n, 24)).astype(np.float32)).to(torch.bfloat16).view(torch.int16).to(dev)
+    T = torch.from_numpy(rng.normal(size=n).astype(np.float32)).to(dev)
+    theta = torch.from_numpy((rng.uniform(-1, 1, NP) * 0.2).astype(np.float32)).to(dev)
+    th16 = torch.empty(NP, dtype=torch.int16, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+    assert L.jq_mlp_sync_bf16(theta.data_ptr(), th16.data_ptr(), st) == 0
+    idx = torch.from_numpy(rng.integers(0, n, size=batch).astype(np.int32)).to(dev)
+    scratch = torch.empty(L.jq_mlp_scratch_floats(ctas), dtype=torch.float32, device=dev)
+    g_r, g_n = torch.empty(NP, device=dev), torch.empty(NP, device=dev)
+    l_r, l_n = torch.empty(1, device=dev), torch.empty(1, device=dev)
+
+    def args(g, loss, scr, k):  # gradient only: theta stays as it is
+        return StepArgs(theta.data_ptr(), th16.data_ptr(), None, None, X.data_ptr(), T.data_ptr(),
+                        idx.data_ptr(), batch, 1, 1e-3, 0, g.data_ptr(), loss.data_ptr(),
+                        scr.data_ptr() if scr is not None else None, k, st)
+
+    assert L.jq_mlp_train_step(ctypes.byref(args(g_r, l_r, scratch, ctas))) == 0
+    assert L.jq_mlp_train_step_noalloc(ctypes.byref(args(g_n, l_n, None, ctas))) == 0  # loads, resolves
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    alloc0 = torch.cuda.memory_allocated()
+    g_n.zero_()
+    torch.cuda.synchronize()
+    assert L.jq_mlp_train_step_noalloc(ctypes.byref(args(g_n, l_n, None, ctas))) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_allocated() == alloc0
+    assert close(g_n, g_r)
+    assert abs(float(l_n) - float(l_r)) <= 1e-4 * max(1.0, abs(float(l_r)))
+    assert L.jq_mlp_train_step_noalloc(ctypes.byref(args(g_n, l_n, None, 17))) == -6
+    assert L.jq_mlp_train_step_noalloc(None) == -1
