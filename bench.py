@@ -40,7 +40,9 @@ WORKLOADS = {
     "batched": SOC,
     "plain": SOC,
     "timed": SOC + ", per-pin delays U[20,200] ps, setup 30 / hold 10 ps, 10 ns clock, "
-                   "DFF clock arrival U[0,300] ps, arrivals + setup/hold events drained per window",
+                   "DFF clock arrival U[0,300] ps, setup/hold checks per stream, events drained per window",
+    "timed_plain": SOC + ", per-pin delays U[20,200] ps, setup 30 / hold 10 ps, 10 ns clock, "
+                         "DFF clock arrival U[0,300] ps, one stream, arrivals + events drained per window",
     "multi": "12 SoC-family designs, 50k-4M AND nodes log-uniform, X-prop, one graph-captured launch",
 }
 
@@ -494,7 +496,121 @@ def run_mine_batched(args, rank, world):
                 script=s, d=d)
 
 
+def timed_design(args, rank, blocks, target_parts=0):
+    """The SoC netlist with per-AND-pin delays U[20,200] ps (rise = fall),
+    scripted with those delays injected; and its constraint buffer: setup 30
+    / hold 10 ps, 10 ns clock, per-DFF clock arrival U[0,300] ps."""
+    from jacquard_b200 import timing
+    d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
+    rng = np.random.default_rng(3)
+    n = d.num_pins + 1
+    r = rng.integers(20, 201, size=n).astype(np.uint32)
+    r[d.kind != 1] = 0
+    d.set_delays(r, r)
+    s = build_script(d, blocks, target_parts=target_parts)
+    zero = np.zeros(n, np.uint32)
+    d.set_delays(zero, zero)
+    ca = np.random.default_rng(5).integers(0, 301, size=int(d.num_dffs)).astype(np.int16)
+    return d, s, timing.constraint_buffer(d, s, 10_000, 30, 10, ca)
+
+
 def run_mine_timed(args, rank, world):
+    """Timed path, 256 streams on the batched interpreter: arrivals (computed
+    once, they do not depend on the stream) and setup/hold checks per stream.
+    One step = one launch window of cycles plus the drain of its events into
+    per-stream violation counts."""
+    import torch
+    from jacquard_b200 import batched, state, timing
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    d, s, cons = timed_design(args, rank, args.blocks, args.blocks // max(1, args.lanes // 2))
+    lanes = args.lanes
+    streams = 32 * lanes
+    W = args.window
+    assert W % 2 == 0
+    po_sig = state.po_positions(s, d)
+    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
+    cap = args.event_capacity
+    tm = batched.Timing(s, cons, cap, device=dev)
+    stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
+    snap0 = np.zeros((lanes, B.sig), np.uint32)
+    xt = state.xmask_all_state_x(s)
+    rio = s.reg_io_state_size
+    snap0[:, rio * 32:2 * rio * 32] = batched.to_batched(np.repeat(xt[None, :], streams, axis=0))
+    snap0[:, :B.in_sigs] = stim[0]
+    B.load_state(snap0)
+    B.reset_sram(x=True)
+    stim_pin = torch.from_numpy(np.ascontiguousarray(stim).reshape(-1).view(np.int32)).pin_memory()
+    stim_dev = torch.empty(stim_pin.numel(), dtype=torch.int32, device=dev)
+    stim_dev.copy_(stim_pin)
+    wave = torch.empty(W * len(po_sig) * lanes, dtype=torch.int32, device=dev)
+    wave_pin = torch.empty(wave.numel(), dtype=torch.int32).pin_memory()
+    ev_pin = torch.empty(tm.events.numel(), dtype=torch.int32).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+    stats = timing.new_stats()
+    cyc = [0]
+
+    def step(drain):
+        tm.reset_events()
+        B.run(stim_dev, W, wave=wave, stream=stream, timing=tm, first_cycle=cyc[0])
+        cyc[0] += W
+        # the window's records: header, then as many as were written
+        ev_pin[:4].copy_(tm.events[:4], non_blocking=True)
+        stream.synchronize()
+        n = min(int(ev_pin[0]) & 0xFFFFFFFF, cap)
+        if n:
+            ev_pin[4:4 + 8 * n].copy_(tm.events[4:4 + 8 * n], non_blocking=True)
+        wave_pin.copy_(wave, non_blocking=True)
+        stream.synchronize()
+        if drain:
+            recs = ev_pin[4:4 + 8 * n].numpy().view(np.uint32).reshape(-1, 8)
+            timing.count_events(recs, int(ev_pin[0]) & 0xFFFFFFFF, cap, stats, streams)
+
+    for _ in range(args.warmup):
+        step(True)
+    assert B.status(stream) == 0
+    # device-timed: launches back to back, the event buffer reset before each
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as ck:
+        timed_region_edge(world)
+        t0.record(stream)
+        for _ in range(args.steps):
+            tm.reset_events()
+            B.run(stim_dev, W, wave=wave, stream=stream, timing=tm, first_cycle=cyc[0])
+            cyc[0] += W
+        t1.record(stream)
+        timed_region_edge(world)
+    dev_ms = t0.elapsed_time(t1)
+    assert B.status(stream) == 0
+    # end to end: stimulus in, launch, the window's events and outputs out,
+    # drained into the violation counts
+    timed_region_edge(world)
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        stim_dev.copy_(stim_pin, non_blocking=True)
+        step(True)
+    timed_region_edge(world)
+    e2e_ms = (time.perf_counter() - w0) * 1e3
+    assert B.status(stream) == 0
+    script_b, state_b = algorithmic_bytes_per_cycle(s, streams=streams, bit_sliced=True)
+    return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams, clocks=ck.summary(),
+                bytes_per_cycle=script_b + state_b, script_bytes=script_b,
+                kernel_ms=dev_ms / args.steps,
+                h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4, launches_per_step=2,
+                design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
+                            script_mb_per_cycle=script_b / 1e6, rio=rio,
+                            major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
+                            setup_violations=stats["setup_violations"],
+                            hold_violations=stats["hold_violations"],
+                            events_dropped=stats["events_dropped"],
+                            streams_with_violations=int(np.count_nonzero(
+                                stats.get("per_stream_hold", np.zeros(1)) +
+                                stats.get("per_stream_setup", np.zeros(1))))),
+                script=s, d=d)
+
+
+def run_mine_timed_plain(args, rank, world):
     """Timed path on the plain interpreter: the SoC netlist with per-AND-pin
     delays U[20,200] ps (rise = fall), setup 30 / hold 10 ps, 10 ns clock,
     per-DFF clock arrival U[0,300] ps, X-prop, arrivals on.  One step = one
@@ -696,9 +812,13 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--mode", default="batched", choices=["plain", "batched", "timed", "multi"],
-                    help="batched: 256 streams (default); plain: 1 stream; timed: arrivals + "
-                         "setup/hold checks with event drain; multi: 12 designs in one graph-captured launch")
+    ap.add_argument("--mode", default="batched",
+                    choices=["plain", "batched", "timed", "timed_plain", "multi"],
+                    help="batched: 256 streams (default); plain: 1 stream; timed: 256 streams with "
+                         "setup/hold checks and event drain; timed_plain: the same on one stream "
+                         "(arrivals written); multi: 12 designs in one graph-captured launch")
+    ap.add_argument("--event-capacity", type=int, default=1 << 22,
+                    help="timed: event records per window")
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
     ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
@@ -753,7 +873,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     runner = {"batched": run_mine_batched, "plain": run_mine_plain, "timed": run_mine_timed,
-              "multi": run_mine_multi}[args.mode]
+              "timed_plain": run_mine_timed_plain, "multi": run_mine_multi}[args.mode]
     r = runner(args, rank, world)
     total_cycles = r["cycles_per_step"] * r["streams"] * args.steps
     mine_val, e2e_val, dev_ms, _ = replica_throughput(total_cycles, r["dev_ms"],
@@ -769,7 +889,7 @@ def main():
         achieved = r["bytes_per_cycle"] * cyc_per_s / 1e9
         script_gbs = r["script_bytes"] * cyc_per_s / 1e9
         tpc = r.get("traffic_per_cycle")
-        if args.no_cpu or args.mode in ("timed", "multi"):
+        if args.no_cpu or args.mode in ("timed", "timed_plain", "multi"):
             cpu_v, cpu_dt = None, 0.0
         else:
             cpu_v, cpu_dt = cpu_baseline(r["script"], r["d"], cycles=args.cpu_cycles, threads=1)

@@ -146,7 +146,8 @@ int jq_max_blocks(int device, size_t *max_blocks);
  * writes (inputs aside, which come from `stimulus`) keep their snapshot-0
  * value in every cycle, where the plain interpreter keeps each snapshot's
  * host pre-fill; the two agree when every snapshot carries the same pre-fill
- * (the X template).  No timing checks. */
+ * (the X template).  Arrivals are not written into the state (they are the
+ * same for every stream: see arrival_first / arrival_steady). */
 typedef struct {
   size_t num_blocks, num_major_stages;
   const size_t *blocks_start;  /* device */
@@ -199,6 +200,23 @@ typedef struct {
                                   partition is X-capable, and then every such
                                   partition's X offset, metadata word 9, is
                                   S/64 words), 0 for scripts without X */
+  /* Setup/hold checks (timing_constraints NULL: none).  The predicate is the
+   * plain interpreter's (and the reference kernel's,
+   * csrc/kernel_v1_impl.cuh:536-558), applied per stream: a word's arrival
+   * does not depend on the stream, only the clock-enable gate does.  The
+   * arrivals come from two tables of one u32 per state word (low 16 bits):
+   * arrival_first for the first cycle of a launch, arrival_steady for the
+   * others.  They are the arrival sections of snapshots 1 and 2 of a
+   * two-cycle jq_simulate run of the same script with an arrival section
+   * (any stimulus): the plain interpreter's per-block writeout arrivals
+   * start at zero in each launch and repeat from the second cycle on.
+   * Events are the reference's records with `reserved` = the stream
+   * (32 * lane + bit), `cycle` = first_cycle + the cycle in the launch. */
+  const uint32_t *timing_constraints; /* device [clock_ps, state words...] */
+  const uint32_t *arrival_first, *arrival_steady; /* device, state words each */
+  jq_event_buffer *events;     /* device; count/overflow as for jq_simulate */
+  uint32_t event_capacity;
+  uint32_t first_cycle;
 } jq_batch_args;
 
 /* Prepares a script (FlattenedScriptV1, device arrays) for the batched

@@ -28,7 +28,9 @@ class BatchArgs(ctypes.Structure):
                 ("part_cycles", vp), ("part_base", vp), ("gr_sources", vp),
                 ("grid", ctypes.c_size_t),
                 ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp),
-                ("lanes_per_item", ctypes.c_uint32), ("x_interleaved", ctypes.c_int32)]
+                ("lanes_per_item", ctypes.c_uint32), ("x_interleaved", ctypes.c_int32),
+                ("timing_constraints", vp), ("arrival_first", vp), ("arrival_steady", vp),
+                ("events", vp), ("event_capacity", ctypes.c_uint32), ("first_cycle", ctypes.c_uint32)]
 
 
 def lib():
@@ -242,10 +244,11 @@ class BatchedSim:
         return base
 
     def run(self, stim, cycles, wave=None, record_buf=None, stream=None, part_cycles=None,
-            barrier_timeout_cycles=0):
+            barrier_timeout_cycles=0, timing=None, first_cycle=0):
         """stim: device tensor [(cycles+1) * lanes * in_sigs] int32 or None.
         barrier_timeout_cycles: grid-barrier wait limit in SM clocks (0 = the
-        library's default of about a second)."""
+        library's default of about a second).  timing: a Timing (setup/hold
+        checks per stream into its event buffer), or None."""
         L = lib()
         wave_ptr = wave.data_ptr() if wave is not None else None
         a = BatchArgs(self.ds.num_blocks, self.ds.num_major_stages, self.ds.blocks_start.data_ptr(),
@@ -263,6 +266,13 @@ class BatchedSim:
                       self.grid, barrier_timeout_cycles,
                       stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream,
                       self.lanes_per_item, self.x_interleaved)
+        if timing is not None:
+            a.timing_constraints = timing.constraints.data_ptr()
+            a.arrival_first = timing.arrival_first.data_ptr()
+            a.arrival_steady = timing.arrival_steady.data_ptr()
+            a.events = timing.events.data_ptr()
+            a.event_capacity = timing.capacity
+            a.first_cycle = first_cycle
         rc = L.jq_simulate_batched(ctypes.byref(a))
         if rc:
             raise RuntimeError("jq_simulate_batched: " + sim.lib().jq_strerror(rc).decode())
@@ -277,6 +287,48 @@ class BatchedSim:
         out = torch.empty(self.lanes * self.sig, dtype=torch.int32, device=self.device)
         self._convert(lib().jq_batched_unpack_state, src, out)
         return out
+
+
+def arrival_tables(script, device="cuda", stream=None):
+    """The u16 arrival of every state word in the first cycle of a launch
+    and in later cycles (int32 device tensors of reg_io_state_size words):
+    the arrival sections of snapshots 1 and 2 of a two-cycle run of the
+    plain interpreter on the same script.  Arrivals follow from the script's
+    delays and each block's execution order, not from the stimulus, so an
+    all-zero state serves."""
+    rio = script.reg_io_state_size
+    eff = rio * (2 if script.xprop_enabled else 1) + rio  # + arrival section
+    ds = sim.DeviceScript(script, device)
+    st = torch.zeros(3 * eff, dtype=torch.int32, device=device)
+    n_sram = max(1, script.sram_storage_size)
+    sram = torch.zeros(n_sram, dtype=torch.int32, device=device)
+    sram_x = torch.zeros(n_sram, dtype=torch.int32, device=device)
+    off = eff - rio
+    sim.simulate(ds, st, 2, eff, sram, sram_x, arrival_state_offset=off, stream=stream)
+    rc = sim.status(stream)
+    if rc:
+        raise RuntimeError("arrival tables: " + sim.lib().jq_strerror(rc).decode())
+    snaps = st.view(3, eff)
+    return snaps[1, off:].clone(), snaps[2, off:].clone()
+
+
+class Timing:
+    """Setup/hold checking for batched runs: the constraint buffer
+    ([clock_ps, setup << 16 | hold per state word]), the script's arrival
+    tables and an event buffer of `capacity` records (sim.new_event_buffer)."""
+
+    def __init__(self, script, constraints, capacity, device="cuda"):
+        self.constraints = sim.u32_to_dev(np.asarray(constraints, np.uint32), device)
+        self.arrival_first, self.arrival_steady = arrival_tables(script, device)
+        self.capacity = capacity
+        self.events = sim.new_event_buffer(capacity, device)
+
+    def reset_events(self):
+        self.events[:2].zero_()
+
+    def read(self):
+        """(records (n, 8) u32, count, overflow) of the events so far."""
+        return sim.read_events(self.events)
 
 
 class CombinedScript:

@@ -24,8 +24,11 @@
 // compacted global-read slots).  Each script chunk is staged into shared
 // memory with a TMA bulk copy (cp.async.bulk, mbarrier completion,
 // double-buffered one chunk ahead); the global read copies its slots with
-// cp.async.  Timing arrivals / setup-hold events are handled by the plain
-// interpreter (they do not depend on the stimulus stream).
+// cp.async.  Setup/hold checks run per stream in the commit: a word's arrival
+// does not depend on the stream (it follows from the script's delays and
+// each script block's execution order), so the caller computes the arrival
+// tables once with the plain interpreter, and only the clock-enable gate of
+// the check differs between streams.
 #include "sim_common.cuh"
 
 #include <cstdio>
@@ -76,6 +79,13 @@ struct BatchParams {
   const uint32_t *part_base;         // first partition index of (stage, block)
   const uint32_t *gr_sources;        // per partition: source signal of each of
                                      // the 8192 global-read positions
+  // setup/hold checks (null constraints: none): [clock_ps, one u32 per state
+  // word], the u16 arrival of each state word in a launch's first cycle and
+  // in later cycles, the event sink
+  const uint32_t *constraints;
+  const uint32_t *arr_first, *arr_steady;
+  jq_event_buffer *events;
+  uint32_t event_cap, first_cycle;
   uint64_t timeout;        // grid-barrier wait limit (SM clocks)
   uint64_t chunk_timeout;  // script-chunk copy wait limit: fixed, so a short
                            // barrier limit never leaves a copy in flight
@@ -259,6 +269,60 @@ __device__ bool grid_wait(const BatchParams &P, Shared &sh, unsigned long long b
   return sh.ok != 0;
 }
 
+// One event record (csrc/event_buffer.h Event) at index idx of the sink;
+// `reserved` carries the stream.  Past the capacity only the overflow flag.
+__device__ __forceinline__ void put_event(const BatchParams &P, uint32_t idx, uint32_t type,
+                                          uint32_t word, uint32_t cycle, uint32_t slack,
+                                          uint32_t arr, uint32_t cv, uint32_t stream) {
+  if (idx < P.event_cap) {
+    jq_event *e = &P.events->events[idx];
+    e->event_type = type;
+    e->message_id = word;
+    e->cycle = cycle;
+    e->reserved = stream;
+    e->data[0] = word;
+    e->data[1] = slack;
+    e->data[2] = arr;
+    e->data[3] = cv;
+  } else {
+    atomicExch(&P.events->overflow, 1u);
+  }
+}
+
+// Setup/hold check of state word `word` for the streams of lane words l0 and
+// l1 (bit masks m0, m1: the streams whose clock enable is set on any signal
+// of the word), with the same predicate as the plain interpreter
+// (csrc/kernel_v1_impl.cuh:536-558) applied per stream: the word's arrival
+// does not depend on the stream, its clock enable does.  Called by a whole
+// warp with the same arguments; lane j writes the records of stream bit j.
+__device__ void check_word(const BatchParams &P, uint32_t word, uint32_t m0, uint32_t l0,
+                           uint32_t m1, uint32_t l1, uint32_t cycle, bool first) {
+  if (!(m0 | m1)) return;
+  const uint32_t cv = __ldg(P.constraints + 1 + word);
+  if (!cv) return;
+  const uint32_t a = __ldg((first ? P.arr_first : P.arr_steady) + word) & 0xffffu;
+  const uint32_t clock_ps = __ldg(P.constraints);
+  const uint32_t su = cv >> 16, ho = cv & 0xffffu;
+  const uint32_t lane = threadIdx.x & 31, below = (1u << lane) - 1u;
+  const uint32_t n0 = __popc(m0), n = n0 + __popc(m1);
+#pragma unroll
+  for (int kind = 0; kind < 2; ++kind) {
+    const bool v = kind == 0 ? (a > 0 && a + su > clock_ps) : (a < ho);
+    if (!v) continue;
+    const uint32_t type = kind == 0 ? 4u : 5u;
+    const uint32_t slack = kind == 0 ? (uint32_t)((int32_t)clock_ps - (int32_t)a - (int32_t)su)
+                                     : (uint32_t)((int32_t)a - (int32_t)ho);
+    const uint32_t c = kind == 0 ? su : ho;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&P.events->count, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((m0 >> lane) & 1u)
+      put_event(P, base + __popc(m0 & below), type, word, cycle, slack, a, c, 32 * l0 + lane);
+    if ((m1 >> lane) & 1u)
+      put_event(P, base + n0 + __popc(m1 & below), type, word, cycle, slack, a, c, 32 * l1 + lane);
+  }
+}
+
 // One (block, lane) work item: the block's partition list for one lane word.
 // Tree state and writeouts hold (value, X) pairs so one shared-memory access
 // moves both.  The script is in the prepared layout (jq_batched_prepare):
@@ -278,7 +342,8 @@ template <bool DS>
 __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, uint32_t *chunks,
                          uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                          const uint32_t *in, uint32_t *out, uint32_t lane, uint32_t pid0,
-                         bool &failed, unsigned long long &next_ticket, bool &have_next) {
+                         bool &failed, unsigned long long &next_ticket, bool &have_next,
+                         uint32_t cyc) {
   const int t = threadIdx.x;
   // the lane's words: with xhalf (v, x) pairs at 4 * (pair * V + s) + 2 * odd
   // (X-capable partitions always run in the quad layout), else values at
@@ -645,6 +710,9 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
               const uint2 me = WO[q];
               cp[uu] = (src.x & ~set0) ^ inv;
               cpx[uu] = is_x ? (src.y & ~set0) : 0u;
+              if (P.constraints)  // a warp holds the 32 signals of one word
+                check_word(P, io_off + (q >> 5), __reduce_or_sync(0xffffffffu, cp[uu]), lane,
+                           0u, 0u, P.first_cycle + cyc, cyc == 0);
               wv[uu] = me.x ^ dinv;
               wx[uu] = me.y;
               sg[uu] = lane_base + (((size_t)io_off * 32 + q) << sig_shift);
@@ -713,7 +781,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
                           uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                           const uint32_t *in, uint32_t *out, uint32_t lp, uint32_t pid0,
                           bool &failed, unsigned long long &next_ticket, bool &have_next,
-                          bool &pending, unsigned long long &bar_target) {
+                          bool &pending, unsigned long long &bar_target, uint32_t cyc) {
   const int t = threadIdx.x;
   // the pair's words: quads (v0, x0, v1, x1) at 4 * (lp * V + s) with
   // xhalf, else (v0, v1) at 2 * (lp * sig + s)
@@ -1084,6 +1152,10 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
               const uint4 me = WO[q];
               const size_t sg = (size_t)io_off * 32 + q;
               const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
+              if (P.constraints)  // a warp holds the 32 signals of one word
+                check_word(P, io_off + (q >> 5), __reduce_or_sync(0xffffffffu, cp0), 2 * lp,
+                           __reduce_or_sync(0xffffffffu, cp1), 2 * lp + 1, P.first_cycle + cyc,
+                           cyc == 0);
               const uint32_t n0 = (o[uu][0] & ~cp0) | ((me.x ^ dinv) & cp0);
               const uint32_t n1 = (o[uu][1] & ~cp1) | ((me.z ^ dinv) & cp1);
               if (is_x) {
@@ -1312,10 +1384,11 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
         if constexpr (NL == 2)
           run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
                     uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
-                    pending, bar_target);
+                    pending, bar_target, (uint32_t)c);
         else
           run_item<DS>(P, sh, reinterpret_cast<uint2 *>(S), reinterpret_cast<uint2 *>(WO), chunks,
-                       uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next);
+                       uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
+                       (uint32_t)c);
         if (failed) {
           if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
           return;
@@ -1954,6 +2027,13 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.part_base = a->part_base;
   P.gr_sources = a->gr_sources;
   if (!P.part_base || !P.gr_sources) return JQ_ERR_INVALID_ARG;
+  P.constraints = a->timing_constraints;
+  P.arr_first = a->arrival_first;
+  P.arr_steady = a->arrival_steady;
+  P.events = a->events;
+  P.event_cap = a->event_capacity;
+  P.first_cycle = a->first_cycle;
+  if (P.constraints && (!P.arr_first || !P.arr_steady || !P.events)) return JQ_ERR_INVALID_ARG;
   P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
   P.chunk_timeout = DEFAULT_BARRIER_TIMEOUT;
   P.slot = launch_slot(a->stream, true);

@@ -134,6 +134,26 @@ def process_events(events, count, capacity, stats, builder=None, resolver=None):
                              "arrival_ps": arr, "constraint_ps": cons, "slack_ps": slack})
 
 
+def count_events(events, count, capacity, stats, streams=None):
+    """Vectorised drain of a buffer's violation records into `stats` (counts
+    only; for the many records of batched runs).  With `streams`, also
+    per-stream counts: stats['per_stream_setup'] / ['per_stream_hold'],
+    arrays indexed by the records' stream field (`reserved`)."""
+    if count > capacity:
+        stats["events_dropped"] += count - capacity
+    ev = np.asarray(events, dtype=np.uint32).reshape(-1, 8)
+    setup = ev[:, 0] == EVENT_SETUP
+    hold = ev[:, 0] == EVENT_HOLD
+    stats["setup_violations"] += int(setup.sum())
+    stats["hold_violations"] += int(hold.sum())
+    if streams is not None:
+        for kind, sel in (("setup", setup), ("hold", hold)):
+            key = f"per_stream_{kind}"
+            c = np.bincount(ev[sel, 3].astype(np.int64), minlength=streams)[:streams]
+            stats[key] = stats.get(key, np.zeros(streams, np.int64)) + c
+    return stats
+
+
 def constraint_buffer(design, script, clock_ps, setup_ps, hold_ps, clock_arrival_ps):
     """Timing constraint buffer [clock_ps, per-word setup<<16 | hold] for every
     DFF of a design (build_timing_constraint_buffer, src/flatten.rs:1891-1924,

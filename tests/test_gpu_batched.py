@@ -10,13 +10,6 @@ from jacquard_b200 import batched, state
 pytestmark = pytest.mark.gpu
 
 
-def per_stream_states(kind, s, cycles, streams, x_init):
-    out = []
-    for k in range(streams):
-        out.append(cases.stimulus(kind, s, cycles, seed=1000 + k, x_init=x_init))
-    return np.stack(out)  # (S, cycles+1, eff)
-
-
 @pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots,per_item,grid", [
     ("tiny", 8, (5,), False, 1, None, 0, 0),
     ("sram", 16, (8,), True, 2, None, 0, 0),     # lane pairs
@@ -154,45 +147,97 @@ def test_layout_roundtrip():
     assert np.array_equal(batched.from_batched(batched.to_batched(a), 5), a)
 
 
-def _batched_inputs(kind, s, cycles, lanes, seed0):
-    S = 32 * lanes
-    snaps = np.stack([cases.stimulus(kind, s, cycles, seed=seed0 + k, x_init=True) for k in range(S)])
-    return batched.to_batched(snaps)  # (cycles+1, lanes, sig)
-
-
-def test_multi_design_single_launch_matches_separate_runs():
+def test_multi_design_single_launch_matches_oracle():
     """Three designs of uneven size relocated into one script share one
-    persistent launch; each design's state equals its own separate run."""
+    persistent launch, captured in a CUDA graph and replayed; every snapshot
+    of every stream of every design equals the oracle's run of that design
+    and stream alone, and so do the SRAM contents."""
     specs = [("tiny", 8, (5,)), ("sram", 16, (8,)), ("soc_mini", 148, (20, 40, 60))]
     scripts = [cases.script(k, nb, sp, xprop=True) for k, nb, sp in specs]
     lanes, cycles = 1, 8
-    bts = [_batched_inputs(k, s, cycles, lanes, 500 + 37 * i)
-           for i, ((k, _, _), s) in enumerate(zip(specs, scripts))]
-    finals = []
-    for s, bt in zip(scripts, bts):
-        B = batched.BatchedSim(s, lanes)
-        B.load_state(bt[0])
-        B.reset_sram()
-        stim = torch.from_numpy(np.ascontiguousarray(bt[:, :, :B.in_sigs]).reshape(-1).view(np.int32)).cuda()
-        B.run(stim, cycles)
-        assert B.status() == 0
-        finals.append(B.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, -1))
+    S = 32 * lanes
+    snaps = [np.stack([cases.stimulus(k, s, cycles, seed=500 + 37 * i + j, x_init=True)
+                       for j in range(S)]) for i, ((k, _, _), s) in enumerate(zip(specs, scripts))]
     C = batched.CombinedScript(scripts)
-    BC = batched.BatchedSim(C, lanes)
+    BC = batched.BatchedSim(C, lanes, record=True)
+    bts = [batched.to_batched(sn) for sn in snaps]  # (cycles+1, lanes, sig_d)
     snap0 = C.combine_states([bt[0] for bt in bts])
     assert snap0.shape == (lanes, BC.sig)
     BC.load_state(snap0)
     BC.reset_sram()
     stim = np.concatenate([bt[:, :, :batched.input_words(s) * 32] for s, bt in zip(scripts, bts)], axis=-1)
     stim_d = torch.from_numpy(np.ascontiguousarray(stim).reshape(-1).view(np.int32)).cuda()
-    # capture the launch in a CUDA graph and replay it
+    rec = torch.zeros((cycles + 1) * lanes * BC.sig, dtype=torch.int32, device="cuda")
+    rec[:lanes * BC.sig].copy_(torch.from_numpy(np.ascontiguousarray(snap0).reshape(-1).view(np.int32)))
     g = torch.cuda.CUDAGraph()
     torch.cuda.synchronize()
     with torch.cuda.graph(g):
-        BC.run(stim_d, cycles)
+        BC.run(stim_d, cycles, record_buf=rec)
     g.replay()
     torch.cuda.synchronize()
     assert BC.status() == 0
-    got = BC.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, -1)
+    got_all = rec.cpu().numpy().view(np.uint32).reshape(cycles + 1, lanes, BC.sig)
+    sram = BC.sram.cpu().numpy().view(np.uint32).reshape(S, -1)
     for d, s in enumerate(scripts):
-        assert np.array_equal(C.design_state(d, got), finals[d]), f"design {d}"
+        eff = snaps[d].shape[-1]
+        got = batched.from_batched(C.design_state(d, got_all), eff)  # (S, cycles+1, eff)
+        n_sram = max(1, s.sram_storage_size)
+        for k in range(S):
+            want = snaps[d][k].reshape(-1).copy()
+            osram = np.zeros(n_sram, np.uint32)
+            osram_x = np.full(n_sram, 0xFFFFFFFF, np.uint32)
+            oracle_lib.simulate(s, want, cycles, eff, sram=osram, sram_x=osram_x)
+            assert np.array_equal(got[k].reshape(-1), want), f"design {d} stream {k}"
+            if s.sram_storage_size:
+                b = C.sram_base[d]
+                assert np.array_equal(sram[k, b:b + s.sram_storage_size], osram[:s.sram_storage_size])
+
+
+@pytest.mark.parametrize("xprop,lanes,per_item", [(False, 2, 2), (True, 2, 2), (True, 1, 1)])
+def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item):
+    """Setup/hold checks in the batched interpreter, two launch windows of 12
+    cycles: every stream's snapshots, and the multiset of (stream, event)
+    records over all streams, equal the oracle's run of each stream with the
+    same windows (per-block writeout arrivals restart with each launch)."""
+    s = cases.script("sram", 16, (8,), xprop=xprop, timing_seed=9)
+    cons = cases.constraint_buffer("sram", s, clock_ps=120, setup=30, hold=150)
+    S, win, nwin = 32 * lanes, 12, 2
+    cycles = win * nwin
+    snaps = np.stack([cases.stimulus("sram", s, cycles, seed=700 + k, x_init=xprop)
+                      for k in range(S)])
+    eff = snaps.shape[-1]
+    want_ev = []
+    want = snaps.copy()
+    for k in range(S):
+        st = want[k].reshape(-1)
+        sram = np.zeros(max(1, s.sram_storage_size), np.uint32)
+        sram_x = np.full_like(sram, 0xFFFFFFFF)
+        for w in range(nwin):
+            ev, cnt = oracle_lib.simulate(s, st[w * win * eff:], win, eff, sram=sram, sram_x=sram_x,
+                                          constraints=cons, event_cap=1 << 14)
+            r = ev.view(np.uint32).reshape(-1, 8).copy()
+            assert cnt == r.shape[0]
+            r[:, 2] += w * win
+            r[:, 3] = k
+            want_ev.append(r)
+    want_ev = np.concatenate(want_ev)
+    assert set(want_ev[:, 0].tolist()) == {4, 5}
+
+    B = batched.BatchedSim(s, lanes, record=True, lanes_per_item=per_item)
+    tm = batched.Timing(s, cons, capacity=1 << 17)
+    bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
+    B.load_state(bt[0])
+    B.reset_sram()
+    got = []
+    for w in range(nwin):
+        rows = bt[w * win:(w + 1) * win + 1, :, :B.in_sigs]
+        stim = torch.from_numpy(np.ascontiguousarray(rows).reshape(-1).view(np.int32)).cuda()
+        rec = torch.zeros((win + 1) * B.sig * lanes, dtype=torch.int32, device="cuda")
+        B.run(stim, win, record_buf=rec, timing=tm, first_cycle=w * win)
+        assert B.status() == 0
+        g = batched.from_batched(rec.cpu().numpy().view(np.uint32).reshape(win + 1, lanes, B.sig), eff)
+        for k in range(S):
+            assert np.array_equal(g[k][1:], want[k][w * win + 1:(w + 1) * win + 1]), f"window {w} stream {k}"
+    recs, count, overflow = tm.read()
+    assert overflow == 0 and count == want_ev.shape[0]
+    assert sorted(map(tuple, recs.tolist())) == sorted(map(tuple, want_ev.tolist()))
