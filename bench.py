@@ -428,7 +428,7 @@ def run_mine_batched(args, rank, world):
     W = args.window
     assert W % 2 == 0, "even windows keep the final state in buffer A"
     po_sig = state.po_positions(s, d)
-    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig, threads=args.threads)
+    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
     # snapshot 0: inputs of cycle 0, every DFF/SRAM word X
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
     snap0 = np.zeros((lanes, B.sig), np.uint32)
@@ -490,7 +490,6 @@ def run_mine_batched(args, rank, world):
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
-                            threads_per_cta=B.threads,
                             partitioner="balanced: at most %d per major stage%s"
                             % (args.blocks // max(1, args.lanes // 2),
                                ", learned refinement" if model is not None else "")),
@@ -530,7 +529,7 @@ def run_mine_timed(args, rank, world):
     W = args.window
     assert W % 2 == 0
     po_sig = state.po_positions(s, d)
-    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig, threads=args.threads)
+    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
     cap = args.event_capacity
     tm = batched.Timing(s, cons, cap, device=dev)
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
@@ -823,9 +822,6 @@ def main():
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
     ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
-    ap.add_argument("--threads", type=int, default=None, choices=[512, 1024],
-                    help="batched: threads per CTA (default: 1024 for scripts in the compact "
-                         "form, else 512)")
     ap.add_argument("--cpu-cycles", type=int, default=160,
                     help="CPU baseline sample: cycles of one stream (about 10 s single-threaded)")
     ap.add_argument("--clusters", type=int, default=512,

@@ -217,11 +217,6 @@ typedef struct {
   jq_event_buffer *events;     /* device; count/overflow as for jq_simulate */
   uint32_t event_capacity;
   uint32_t first_cycle;
-  uint32_t threads_per_cta;    /* 0 or 512; or 1024: lane-pair items run by 32
-                                  warps, for scripts whose partitions all
-                                  have the compact form (jq_batched_all_compact);
-                                  a partition in the tree form then ends the
-                                  launch with JQ_ERR_INVALID_ARG as its status */
 } jq_batch_args;
 
 /* Prepares a script (FlattenedScriptV1, device arrays) for the batched
@@ -242,11 +237,6 @@ int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
                        size_t num_partitions, uint32_t *out, uint32_t *part_base,
                        uint32_t *gr_sources, void *stream);
 int jq_simulate_batched(const jq_batch_args *a);
-/* Device word *flag <- 1 when every partition of a script prepared by
- * jq_batched_prepare is in the compact form (every boomerang stage of it
- * evaluates tree level 1 only), else 0; asynchronous on `stream`. */
-int jq_batched_all_compact(const size_t *blocks_start, const uint32_t *prepared, size_t num_blocks,
-                           size_t num_major_stages, uint32_t *flag, void *stream);
 /* Words of one batched state buffer. */
 size_t jq_batched_state_words(uint32_t lanes, size_t signals);
 /* Lane-major [lanes][signals] (device) <-> batched state layout (device),

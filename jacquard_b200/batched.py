@@ -30,8 +30,7 @@ class BatchArgs(ctypes.Structure):
                 ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp),
                 ("lanes_per_item", ctypes.c_uint32), ("x_interleaved", ctypes.c_int32),
                 ("timing_constraints", vp), ("arrival_first", vp), ("arrival_steady", vp),
-                ("events", vp), ("event_capacity", ctypes.c_uint32), ("first_cycle", ctypes.c_uint32),
-                ("threads_per_cta", ctypes.c_uint32)]
+                ("events", vp), ("event_capacity", ctypes.c_uint32), ("first_cycle", ctypes.c_uint32)]
 
 
 def lib():
@@ -48,8 +47,6 @@ def lib():
         L.jq_batched_prepare.restype = ctypes.c_int
         L.jq_batched_prepare.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
                                          ctypes.c_size_t, vp, vp, vp, vp]
-        L.jq_batched_all_compact.restype = ctypes.c_int
-        L.jq_batched_all_compact.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp, vp]
         L.jq_batched_state_words.restype = ctypes.c_size_t
         L.jq_batched_state_words.argtypes = [ctypes.c_uint32, ctypes.c_size_t]
         for fn in (L.jq_batched_pack_state, L.jq_batched_unpack_state):
@@ -152,7 +149,7 @@ class BatchedSim:
     """Script + buffers on the device for `lanes` lane words (32*lanes streams)."""
 
     def __init__(self, script, lanes, device="cuda", record=False, po_signals=None, grid=0,
-                 wo_slots=None, lanes_per_item=0, threads=None):
+                 wo_slots=None, lanes_per_item=0):
         self.script = script
         self.lanes = lanes
         self.device = torch.device(device)
@@ -214,22 +211,6 @@ class BatchedSim:
         # lane words per work item: 0 lets the library pick (lane pairs when
         # lanes is even and they fit), 1 or 2 forces one
         self.lanes_per_item = lanes_per_item
-        # threads per CTA: 1024 (32 warps per lane-pair item) when every
-        # partition is in the compact form and lane pairs run, else 512;
-        # None picks, 512 or 1024 forces
-        flag = torch.zeros(1, dtype=torch.int32, device=self.device)
-        rc = L.jq_batched_all_compact(self.ds.blocks_start.data_ptr(), self.prepared.data_ptr(),
-                                      self.ds.num_blocks, self.ds.num_major_stages,
-                                      flag.data_ptr(),
-                                      torch.cuda.current_stream(self.device).cuda_stream)
-        if rc:
-            raise RuntimeError("jq_batched_all_compact: " + sim.lib().jq_strerror(rc).decode())
-        self.all_compact = bool(int(flag.item()))
-        pairs = lanes_per_item == 2 or (lanes_per_item == 0 and lanes % 2 == 0)
-        self._auto_threads = threads is None
-        if threads is None:
-            threads = 1024 if (self.all_compact and pairs) else 512
-        self.threads = threads
 
     def _convert(self, fn, src, dst):
         st = torch.cuda.current_stream(self.device).cuda_stream
@@ -285,7 +266,6 @@ class BatchedSim:
                       self.grid, barrier_timeout_cycles,
                       stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream,
                       self.lanes_per_item, self.x_interleaved)
-        a.threads_per_cta = self.threads
         if timing is not None:
             a.timing_constraints = timing.constraints.data_ptr()
             a.arrival_first = timing.arrival_first.data_ptr()
@@ -294,10 +274,6 @@ class BatchedSim:
             a.event_capacity = timing.capacity
             a.first_cycle = first_cycle
         rc = L.jq_simulate_batched(ctypes.byref(a))
-        if rc == -1 and self._auto_threads and self.threads == 1024:
-            # lane pairs of 32 warps do not fit this script's writeouts
-            self.threads = a.threads_per_cta = 512
-            rc = L.jq_simulate_batched(ctypes.byref(a))
         if rc:
             raise RuntimeError("jq_simulate_batched: " + sim.lib().jq_strerror(rc).decode())
 

@@ -247,7 +247,7 @@ template <class F>
 __device__ bool grid_wait(const BatchParams &P, Shared &sh, unsigned long long bar_target,
                           F &&others) {
   const int t = threadIdx.x;
-  if (t >= 32) others((uint32_t)t - 32, blockDim.x - 32);
+  if (t >= 32) others((uint32_t)t - 32, (uint32_t)BT - 32);
   if (t == 0) {
     int ok = 1;
     uint64_t t0 = clock64();
@@ -777,7 +777,6 @@ __device__ __forceinline__ uint4 shfl4_xor(uint4 v, uint32_t m) {
 // the barriers and the load latencies of a stage are shared by both lane
 // words.  The tree state is single-buffered (128 KB), so a barrier separates
 // the gathers of a stage from its first writes.
-template <int T>
 __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO, uint32_t *chunks,
                           uint32_t &uses0, uint32_t &uses1, const uint32_t *script,
                           const uint32_t *in, uint32_t *out, uint32_t lp, uint32_t pid0,
@@ -795,12 +794,11 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     // its start, or from the end of the barrier wait it took over
     long long t_start = clock64();
     if (t < 256) sh.meta[t] = __ldg(script + off + t);
-    constexpr int GRK = 8192 / T;  // global-read slots per thread
-    uint32_t e[GRK];
+    uint32_t e[16];
     {
       const uint32_t *src = P.gr_sources + (size_t)pid * 8192;
 #pragma unroll
-      for (int k = 0; k < GRK; ++k) e[k] = __ldg(src + t + T * k);
+      for (int k = 0; k < 16; ++k) e[k] = __ldg(src + t + BT * k);
     }
     __syncthreads();
     const uint32_t ns = sh.meta[0];
@@ -841,9 +839,9 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     // registers in two halves of 8 positions.
     if (P.xhalf && is_x) {
 #pragma unroll
-      for (int k = 0; k < GRK; ++k) {
+      for (int k = 0; k < 16; ++k) {
         const uint32_t ek = e[k];
-        uint4 *dst = &S[sw(t + T * k)];
+        uint4 *dst = &S[sw(t + BT * k)];
         if (ek < GR_SKIP) {
           const uint32_t *bp = (ek >> 31) ? out : in;
           const uint32_t *src = bp + pair_base + ((size_t)(ek & 0x7fffffffu) << 2);
@@ -856,12 +854,11 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
       asm volatile("cp.async.wait_all;" ::: "memory");
     } else {
 #pragma unroll
-    constexpr int GH = T == BT ? 8 : 4;  // loads in flight per group (registers)
-    for (int h = 0; h < GRK / GH; ++h) {
-      uint4 v[GH];
+    for (int h = 0; h < 2; ++h) {
+      uint4 v[8];
 #pragma unroll
-      for (int k = 0; k < GH; ++k) {
-        const uint32_t ek = e[GH * h + k];
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t ek = e[8 * h + k];
         v[k] = make_uint4(0, 0, 0, 0);
         if (ek < GR_SKIP) {
           const uint32_t *bp = (ek >> 31) ? out : in;
@@ -877,19 +874,18 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         }
       }
 #pragma unroll
-      for (int k = 0; k < GH; ++k)
-        if (e[GH * h + k] != GR_SKIP) S[sw(t + T * (GH * h + k))] = v[k];
+      for (int k = 0; k < 8; ++k)
+        if (e[8 * h + k] != GR_SKIP) S[sw(t + BT * (8 * h + k))] = v[k];
     }
     }
     const uint32_t lane_i = t & 31, warp_i = t >> 5;
     const uint32_t u = residue(t);
     const uint32_t us = sw(u);
-    // writeout hook (stage << 8 | 32-position group) of slot warp_i + NW *
-    // lane_i (lanes 0..256/NW-1; num_ios <= 256), all ones when there is none
-    constexpr uint32_t NW = T / 32;
+    // writeout hook (stage << 8 | 32-position group) of slot warp_i + 16 *
+    // lane_i (lanes 0..15; num_ios <= 256), all ones when there is none
     uint32_t my_hook = 0xffffffffu;
-    if (lane_i < 256 / NW && warp_i + NW * lane_i < num_ios) {
-      const uint32_t slot = warp_i + NW * lane_i;
+    if (lane_i < 16 && warp_i + 16 * lane_i < num_ios) {
+      const uint32_t slot = warp_i + 16 * lane_i;
       const uint32_t hw = sh.meta[128 + slot / 2];
       my_hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
     }
@@ -922,7 +918,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
   for (uint32_t hm = __ballot_sync(0xffffffffu, (my_hook >> 8) == (stage)); hm; hm &= hm - 1) { \
     const uint32_t j = __ffs(hm) - 1;                                                         \
     const uint32_t blk = __shfl_sync(0xffffffffu, my_hook, j) & 255u;                         \
-    WO[(warp_i + NW * j) * 32 + lane_i] = S[(pbase) + 32 * blk + lane_i];                     \
+    WO[(warp_i + 16 * j) * 32 + lane_i] = S[(pbase) + 32 * blk + lane_i];                     \
   }
       if (compact && ci == ns && ok) JQ_HOOKS_COMPACT(ns - 1, prev_base)
       if (ci < ns && compact) {
@@ -936,21 +932,18 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
     r = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u), 0u - ((en >> 28) & 1u)); \
   }
         const uint32_t ov = ok ? C[2] : 0u;  // held slots (stage 0)
-        // n <= 4096 slots (CK per thread); held slots ov <= 2048 (HK per thread)
-        constexpr int CK = 4096 / T, HK = 2048 / T;
-        uint4 h[HK];
-#pragma unroll
-        for (int k = 0; k < HK; ++k) h[k] = make_uint4(0, 0, 0, 0);
+        uint4 h[4] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
         if (ok) {
           if (ci > 0) JQ_HOOKS_COMPACT(ci - 1, prev_base)
+          // n <= 4096 slots: at most 8 per thread
 #pragma unroll
-          for (int k = 0; k < CK; ++k) {
-            const uint32_t i = t + T * k;
+          for (int k = 0; k < 8; ++k) {
+            const uint32_t i = t + BT * k;
             if (i >= n) break;
             uint4 r;
             JQ_COMPACT_EVAL(i, r)
-            if (k < HK && i < ov)
-              h[k < HK ? k : 0] = r;
+            if (k < 4 && i < ov)
+              h[k < 4 ? k : 0] = r;
             else
               S[base + i] = r;
           }
@@ -958,18 +951,12 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         JQ_FAIL_IF(!ok)
         if (ov) {
 #pragma unroll
-          for (int k = 0; k < HK; ++k)
-            if (t + T * k < ov) S[base + t + T * k] = h[k];
+          for (int k = 0; k < 4; ++k)
+            if (t + BT * k < ov) S[base + t + BT * k] = h[k];
           __syncthreads();
         }
 #undef JQ_COMPACT_EVAL
         prev_base = base;
-      } else if (ci < ns && T != BT) {
-        // the tree form assumes 512 threads (the thread-major chunk layout
-        // of jq_batched_prepare): a script with such a partition is run by
-        // the 512-thread variant
-        if (t == 0) atomicCAS(&g_status[P.slot], 0, JQ_ERR_INVALID_ARG);
-        JQ_FAIL_IF(true)
       } else if (ci < ns) {
         // ---------------- boomerang stage ci
         uint4 v1[8];
@@ -977,7 +964,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         bool shallow = false, flat = false;  // no position below 512 / 4096 live
         if (ok) {
           const uint4 *P4 = reinterpret_cast<const uint4 *>(C);
-          const uint4 pa = P4[t], pb = P4[(T == BT ? T : 0) + t];
+          const uint4 pa = P4[t], pb = P4[BT + t];
           const uint2 fl = reinterpret_cast<const uint2 *>(C + 4096)[t];
           A = fl.x;
           B = fl.y;
@@ -1069,7 +1056,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         for (uint32_t hm = __ballot_sync(0xffffffffu, (my_hook >> 8) == ci); hm; hm &= hm - 1) {
           const uint32_t j = __ffs(hm) - 1;
           const uint32_t g = __shfl_sync(0xffffffffu, my_hook, j) & 255u;
-          WO[(warp_i + NW * j) * 32 + lane_i] = S[sw(g * 32 + lane_i)];
+          WO[(warp_i + 16 * j) * 32 + lane_i] = S[sw(g * 32 + lane_i)];
         }
       } else if (has_sram && ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports
@@ -1077,7 +1064,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         uint4 *St = S;
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
-        for (uint32_t q = t; q < nq; q += T) {
+        for (uint32_t q = t; q < nq; q += BT) {
           const uint4 w = WO[perm_lin(C, q)];
           const uint4 fl = F4[q >> 5];
           const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q);
@@ -1087,7 +1074,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         __syncthreads();
         // one warp per (SRAM, lane word of the pair), lane = stream
         const int warp = t >> 5, ln = t & 31;
-        for (uint32_t ih = warp; ih < num_srams * 2; ih += T / 32) {
+        for (uint32_t ih = warp; ih < num_srams * 2; ih += BT / 32) {
           const uint32_t i = ih >> 1, hsel = ih & 1;
           const uint32_t *Aw = reinterpret_cast<const uint32_t *>(St + (4 * i) * 32) + 2 * hsel;
           // signal words k of the SRAM's staged rows (read address 0..15,
@@ -1119,7 +1106,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           *reinterpret_cast<uint2 *>(WOw + 4 * (slotw + ln) + 2 * hsel) =
               make_uint2(word, is_x ? wordx : 0u);
         }
-        for (uint32_t q = t; q < num_dup * 32; q += T)
+        for (uint32_t q = t; q < num_dup * 32; q += BT)
           WO[(num_ios - num_srams - num_dup) * 32 + q] = St[num_srams * 4 * 32 + q];
         __syncthreads();
       } else {
@@ -1133,11 +1120,11 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         const uint32_t nq = num_ios * 32;
         // the old words of up to 4 q per thread are loaded before any store,
         // so their latencies overlap
-        for (uint32_t q0 = t; q0 < nq; q0 += 2 * T) {
+        for (uint32_t q0 = t; q0 < nq; q0 += 2 * BT) {
           uint32_t o[2][4];  // old v0, v1, x0, x1
 #pragma unroll
           for (int uu = 0; uu < 2; ++uu) {
-            const uint32_t q = q0 + uu * T;
+            const uint32_t q = q0 + uu * BT;
             if (q < nq) {
               const size_t sg = (size_t)io_off * 32 + q;
               if (is_x) {  // quad layout
@@ -1156,7 +1143,7 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           }
 #pragma unroll
           for (int uu = 0; uu < 2; ++uu) {
-            const uint32_t q = q0 + uu * T;
+            const uint32_t q = q0 + uu * BT;
             if (q < nq) {
               const uint4 src = WO[perm_lin(C, q)];
               const uint4 fl = F4[q >> 5];
@@ -1267,10 +1254,9 @@ __device__ void prefetch_global_read_l2(const BatchParams &P, const Shared &sh, 
 }
 
 // NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
-template <bool DS, int NL, int T>
-__global__ void __launch_bounds__(T, 1) jq_batched_kernel(BatchParams P) {
+template <bool DS, int NL>
+__global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   static_assert(NL == 1 || (NL == 2 && !DS), "lane pairs use a single tree buffer");
-  static_assert(T == BT || NL == 2, "only lane-pair items run with more threads");
   extern __shared__ __align__(128) uint8_t dyn[];
   __shared__ Shared sh;
   constexpr size_t WB = NL == 2 ? 16 : 8;  // bytes per tree / writeout word
@@ -1283,7 +1269,7 @@ __global__ void __launch_bounds__(T, 1) jq_batched_kernel(BatchParams P) {
     mbar_init(&sh.bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (uint32_t q = t; q < P.wo_slots * 32 * (uint32_t)(WB / 4); q += T)
+  for (uint32_t q = t; q < P.wo_slots * 32 * (uint32_t)(WB / 4); q += BT)
     reinterpret_cast<uint32_t *>(WO)[q] = 0;
   // item table: thread ms resolves major stage ms
   if (t == 0) sh.script_words = P.blocks_start[(size_t)P.num_major_stages * P.num_blocks];
@@ -1334,8 +1320,8 @@ __global__ void __launch_bounds__(T, 1) jq_batched_kernel(BatchParams P) {
       // stimulus signals [src, src+count) to state signals [dst, dst+count)
       // (one region at 0 when no list is given)
       const uint32_t *src = P.stim + (c + 1) * P.input_sigs * P.lanes;
-      for (size_t q = (size_t)blockIdx.x * T + t; q < P.input_sigs * P.lanes;
-           q += (size_t)gridDim.x * T) {
+      for (size_t q = (size_t)blockIdx.x * BT + t; q < P.input_sigs * P.lanes;
+           q += (size_t)gridDim.x * BT) {
         const size_t l = q / P.input_sigs, i = q % P.input_sigs;
         size_t dst = i;
         if (P.input_regions) {
@@ -1396,15 +1382,15 @@ __global__ void __launch_bounds__(T, 1) jq_batched_kernel(BatchParams P) {
           else if (t < 256 + 48) prefetch_l2(nscr + 32 * (t - 256));  // metadata, chunk 0 head
         }
         if constexpr (NL == 2)
-          run_item2<T>(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
+          run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
                     uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
                     pending, bar_target, (uint32_t)c);
         else
           run_item<DS>(P, sh, reinterpret_cast<uint2 *>(S), reinterpret_cast<uint2 *>(WO), chunks,
                        uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
                        (uint32_t)c);
-        if (failed) {  // the first recorded error stands
-          if (t == 0) atomicCAS(&g_status[P.slot], 0, JQ_ERR_BARRIER_TIMEOUT);
+        if (failed) {
+          if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
           return;
         }
       }
@@ -1437,14 +1423,14 @@ __global__ void __launch_bounds__(T, 1) jq_batched_kernel(BatchParams P) {
       }
     }
     // record outputs of this cycle
-    for (size_t q = (size_t)blockIdx.x * T + t; q < (size_t)P.n_po * P.lanes;
-         q += (size_t)gridDim.x * T) {
+    for (size_t q = (size_t)blockIdx.x * BT + t; q < (size_t)P.n_po * P.lanes;
+         q += (size_t)gridDim.x * BT) {
       const uint32_t po = (uint32_t)(q / P.lanes), l = (uint32_t)(q % P.lanes);
       P.wave[(c * P.n_po + po) * P.lanes + l] = ldcg(out + phys(P, l, P.po_sig[po]));
     }
     if (P.record) {  // lane-major [lane][signal]
       uint32_t *dst = P.record + (c + 1) * snap;
-      for (size_t q = (size_t)blockIdx.x * T + t; q < snap; q += (size_t)gridDim.x * T)
+      for (size_t q = (size_t)blockIdx.x * BT + t; q < snap; q += (size_t)gridDim.x * BT)
         dst[q] = ldcg(out + phys(P, (uint32_t)(q / P.sig_per_snap), q % P.sig_per_snap));
     }
     // the recording reads `out`; the next cycle writes into `in`: the next
@@ -1829,23 +1815,6 @@ __global__ void jq_batched_count_kernel(const size_t *blocks_start, const uint32
   counts[e] = n;
 }
 
-// Clears *flag when any partition of a prepared script is not in the
-// compact form (metadata word 10, bit 0); one thread per (major stage,
-// block) entry.
-__global__ void jq_batched_compact_kernel(const size_t *blocks_start, const uint32_t *prep,
-                                          unsigned entries, uint32_t *flag) {
-  const unsigned e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= entries) return;
-  size_t off = blocks_start[e];
-  for (;;) {
-    const uint32_t ns = prep[off];
-    if (!ns) break;
-    if (!(prep[off + 10] & 1u)) atomicExch(flag, 0u);
-    if (prep[off + 1]) break;
-    off += 256 + 512 * (size_t)prep[off + 6] + STAGE_WORDS * ((size_t)ns + 2);
-  }
-}
-
 }  // namespace jqk
 
 using namespace jqk;
@@ -1876,17 +1845,13 @@ extern "C" {
 
 // Kernel variant: lane words per work item and tree-state buffering.
 struct Variant {
-  int nl;       // 1 or 2 lane words per item
-  bool ds;      // double-buffered tree state (nl == 1 only)
-  int threads;  // threads per CTA: 512, or 1024 (lane pairs, compact scripts)
+  int nl;   // 1 or 2 lane words per item
+  bool ds;  // double-buffered tree state (nl == 1 only)
 };
 
 static const void *variant_fn(Variant v) {
-  if (v.nl == 2)
-    return v.threads == 1024 ? (const void *)jq_batched_kernel<false, 2, 1024>
-                             : (const void *)jq_batched_kernel<false, 2, BT>;
-  return v.ds ? (const void *)jq_batched_kernel<true, 1, BT>
-              : (const void *)jq_batched_kernel<false, 1, BT>;
+  if (v.nl == 2) return (const void *)jq_batched_kernel<false, 2>;
+  return v.ds ? (const void *)jq_batched_kernel<true, 1> : (const void *)jq_batched_kernel<false, 1>;
 }
 
 static size_t smem_layout_bytes(uint32_t wo_slots, Variant v) {
@@ -1907,18 +1872,11 @@ static bool variant_fits(uint32_t wo_slots, Variant v) {
 // want_nl 0 = automatic: lane pairs when the lane count is even and their
 // shared memory fits, else single lanes, double-buffered when that fits.
 // nl = 0 in the result: the requested variant is not possible.
-// threads 1024 asks for the 32-warp lane-pair variant (nl = 0 when lane
-// pairs are not possible).
-static Variant pick_variant(uint32_t wo_slots, uint32_t lanes, uint32_t want_nl,
-                            uint32_t threads = BT) {
-  if (threads == 1024) {
-    const Variant v{2, false, 1024};
-    return want_nl != 1 && lanes % 2 == 0 && variant_fits(wo_slots, v) ? v : Variant{0, false, 0};
-  }
-  if (want_nl != 1 && lanes % 2 == 0 && variant_fits(wo_slots, Variant{2, false, BT}))
-    return Variant{2, false, BT};
-  if (want_nl == 2) return Variant{0, false, BT};
-  return Variant{1, variant_fits(wo_slots, Variant{1, true, BT}), BT};
+static Variant pick_variant(uint32_t wo_slots, uint32_t lanes, uint32_t want_nl) {
+  if (want_nl != 1 && lanes % 2 == 0 && variant_fits(wo_slots, Variant{2, false}))
+    return Variant{2, false};
+  if (want_nl == 2) return Variant{0, false};
+  return Variant{1, variant_fits(wo_slots, Variant{1, true})};
 }
 
 int jq_batched_smem_bytes(uint32_t wo_slots) {
@@ -1932,7 +1890,7 @@ static int variant_max_blocks(int device, uint32_t wo_slots, Variant v, size_t *
     return JQ_ERR_LAUNCH;
   int sms = 0, per = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, v.threads, smem) != cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, BT, smem) != cudaSuccess)
     return JQ_ERR_LAUNCH;
   *max_blocks = (size_t)sms * per;
   return JQ_OK;
@@ -2022,20 +1980,6 @@ int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
   return rc;
 }
 
-int jq_batched_all_compact(const size_t *blocks_start, const uint32_t *prepared, size_t num_blocks,
-                           size_t num_major_stages, uint32_t *flag, void *stream) {
-  if (!blocks_start || !prepared || !flag || num_blocks == 0 || num_major_stages == 0)
-    return JQ_ERR_INVALID_ARG;
-  cudaStream_t st = (cudaStream_t)stream;
-  static const uint32_t one = 1;
-  if (cudaMemcpyAsync(flag, &one, sizeof(one), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return JQ_ERR_CUDA;
-  const size_t entries = num_blocks * num_major_stages;
-  jq_batched_compact_kernel<<<(unsigned)((entries + 255) / 256), 256, 0, st>>>(
-      blocks_start, prepared, (unsigned)entries, flag);
-  return cudaGetLastError() == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
-}
-
 int jq_simulate_batched(const jq_batch_args *a) {
   if (!a || a->lanes == 0 || a->num_blocks == 0 || a->num_major_stages == 0 ||
       a->num_major_stages > 32 || !a->state_a || !a->state_b || a->wo_slots > 256 ||
@@ -2046,10 +1990,7 @@ int jq_simulate_batched(const jq_batch_args *a) {
   cudaGetDevice(&dev);
   const uint32_t wo_slots = a->wo_slots ? a->wo_slots : 256;
   if (a->lanes_per_item > 2) return JQ_ERR_INVALID_ARG;
-  if (a->threads_per_cta != 0 && a->threads_per_cta != BT && a->threads_per_cta != 1024)
-    return JQ_ERR_INVALID_ARG;
-  const Variant v = pick_variant(wo_slots, a->lanes, a->lanes_per_item,
-                                 a->threads_per_cta ? a->threads_per_cta : BT);
+  const Variant v = pick_variant(wo_slots, a->lanes, a->lanes_per_item);
   if (v.nl == 0) return JQ_ERR_INVALID_ARG;
   size_t maxg = 0;
   if (variant_max_blocks(dev, wo_slots, v, &maxg) != JQ_OK || maxg == 0) return JQ_ERR_LAUNCH;
@@ -2101,8 +2042,7 @@ int jq_simulate_batched(const jq_batch_args *a) {
   if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
   const int smem = (int)smem_layout_bytes(P.wo_slots, v);
   void *args[] = {&P};
-  cudaError_t e =
-      cudaLaunchCooperativeKernel(variant_fn(v), (unsigned)grid, v.threads, args, smem, st);
+  cudaError_t e = cudaLaunchCooperativeKernel(variant_fn(v), (unsigned)grid, BT, args, smem, st);
   return e == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
 }
 

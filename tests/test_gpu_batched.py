@@ -28,36 +28,17 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slo
     check_batched(kind, cases.script(kind, nb, split, xprop=xprop), lanes, wo_slots, per_item, grid)
 
 
-@pytest.mark.parametrize("kind,nb,split,parts,lanes,grid,threads", [
-    ("soc_mini", 148, (20, 40, 60), 37, 2, 0, 512),    # one item per CTA per stage
-    ("soc_mini", 148, (20, 40, 60), 37, 2, 0, 1024),   # 32-warp lane-pair items
-    ("soc_mini", 148, (20, 40, 60), 37, 2, 5, 512),    # tickets
-    ("soc_mini", 148, (20, 40, 60), 37, 4, 5, 1024),
-    ("sram", 16, (8,), 4, 2, 0, 512),
-    ("sram", 16, (8,), 4, 2, 0, 1024),
+@pytest.mark.parametrize("kind,nb,split,parts,lanes,grid", [
+    ("soc_mini", 148, (20, 40, 60), 37, 2, 0),   # one item per CTA per stage
+    ("soc_mini", 148, (20, 40, 60), 37, 2, 5),   # tickets
+    ("sram", 16, (8,), 4, 2, 0),
 ])
-def test_batched_balanced_partitions_match_oracle(kind, nb, split, parts, lanes, grid, threads):
+def test_batched_balanced_partitions_match_oracle(kind, nb, split, parts, lanes, grid):
     """Balanced, flat partitions (every gate at tree level 1, the batched
-    workload's script form) in lane-pair items, by 16 or 32 warps."""
+    workload's script form) in lane-pair items."""
     s = cases.script(kind, nb, split, xprop=True, target_parts=parts)
     assert int(s.features[:, 14].max()) <= 1  # deepest tree level with a gate
-    check_batched(kind, s, lanes, None, 2, grid, threads)
-
-
-def test_tree_form_partition_refused_by_32_warp_items():
-    """A script with tree-form partitions run by the 32-warp variant ends
-    with JQ_ERR_INVALID_ARG as its status (the tree form needs 512 threads),
-    and the 512-thread variant runs it next on the same context."""
-    s = cases.script("sram", 16, (8,), xprop=True)
-    c = BatchedCase("sram", s, 2, per_item=2, threads=1024)
-    assert not c.B.all_compact
-    c.launch()
-    assert c.B.status() == -1
-    c.B.threads = 512
-    c.reset()
-    c.launch()
-    assert c.B.status() == 0
-    c.verify()
+    check_batched(kind, s, lanes, None, 2, grid)
 
 
 class BatchedCase:
@@ -65,8 +46,7 @@ class BatchedCase:
     results: launch() issues it (on any stream), verify() checks every
     snapshot and SRAM word of every stream."""
 
-    def __init__(self, kind, s, lanes, wo_slots=None, per_item=0, grid=0, cycles=10, seed0=1000,
-                 threads=None):
+    def __init__(self, kind, s, lanes, wo_slots=None, per_item=0, grid=0, cycles=10, seed0=1000):
         xprop = s.xprop_enabled
         self.cycles, self.lanes, self.S = cycles, lanes, 32 * lanes
         snaps = np.stack([cases.stimulus(kind, s, cycles, seed=seed0 + k, x_init=xprop)
@@ -82,7 +62,7 @@ class BatchedCase:
             self.want[k] = st.reshape(cycles + 1, self.eff)
             self.wsram.append(sram)
         self.B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots,
-                                    lanes_per_item=per_item, grid=grid, threads=threads)
+                                    lanes_per_item=per_item, grid=grid)
         self.bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
         B = self.B
         self.stim = torch.from_numpy(
@@ -114,10 +94,8 @@ class BatchedCase:
             assert np.array_equal(gs[k][: self.wsram[k].size], self.wsram[k])
 
 
-def check_batched(kind, s, lanes, wo_slots, per_item, grid, threads=None):
-    c = BatchedCase(kind, s, lanes, wo_slots, per_item, grid, threads=threads)
-    if threads is not None:
-        assert c.B.threads == threads
+def check_batched(kind, s, lanes, wo_slots, per_item, grid):
+    c = BatchedCase(kind, s, lanes, wo_slots, per_item, grid)
     c.launch()
     assert c.B.status() == 0
     c.verify()
@@ -215,14 +193,13 @@ def test_multi_design_single_launch_matches_oracle():
                 assert np.array_equal(sram[k, b:b + s.sram_storage_size], osram[:s.sram_storage_size])
 
 
-@pytest.mark.parametrize("xprop,lanes,per_item,parts", [(False, 2, 2, 0), (True, 2, 2, 0),
-                                                         (True, 1, 1, 0), (True, 2, 2, 4)])
-def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item, parts):
+@pytest.mark.parametrize("xprop,lanes,per_item", [(False, 2, 2), (True, 2, 2), (True, 1, 1)])
+def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item):
     """Setup/hold checks in the batched interpreter, two launch windows of 12
     cycles: every stream's snapshots, and the multiset of (stream, event)
     records over all streams, equal the oracle's run of each stream with the
     same windows (per-block writeout arrivals restart with each launch)."""
-    s = cases.script("sram", 16, (8,), xprop=xprop, timing_seed=9, target_parts=parts)
+    s = cases.script("sram", 16, (8,), xprop=xprop, timing_seed=9)
     cons = cases.constraint_buffer("sram", s, clock_ps=120, setup=30, hold=150)
     S, win, nwin = 32 * lanes, 12, 2
     cycles = win * nwin
