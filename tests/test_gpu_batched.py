@@ -193,13 +193,14 @@ def test_multi_design_single_launch_matches_oracle():
                 assert np.array_equal(sram[k, b:b + s.sram_storage_size], osram[:s.sram_storage_size])
 
 
-@pytest.mark.parametrize("xprop,lanes,per_item", [(False, 2, 2), (True, 2, 2), (True, 1, 1)])
-def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item):
+@pytest.mark.parametrize("xprop,lanes,per_item,parts", [(False, 2, 2, 0), (True, 2, 2, 0),
+                                                         (True, 1, 1, 0), (True, 2, 2, 4)])
+def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item, parts):
     """Setup/hold checks in the batched interpreter, two launch windows of 12
     cycles: every stream's snapshots, and the multiset of (stream, event)
     records over all streams, equal the oracle's run of each stream with the
     same windows (per-block writeout arrivals restart with each launch)."""
-    s = cases.script("sram", 16, (8,), xprop=xprop, timing_seed=9)
+    s = cases.script("sram", 16, (8,), xprop=xprop, timing_seed=9, target_parts=parts)
     cons = cases.constraint_buffer("sram", s, clock_ps=120, setup=30, hold=150)
     S, win, nwin = 32 * lanes, 12, 2
     cycles = win * nwin
@@ -224,7 +225,7 @@ def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_ite
     assert set(want_ev[:, 0].tolist()) == {4, 5}
 
     B = batched.BatchedSim(s, lanes, record=True, lanes_per_item=per_item)
-    tm = batched.Timing(s, cons, capacity=1 << 17)
+    tm = batched.Timing(s, cons, capacity=want_ev.shape[0] + 1024)
     bt = batched.to_batched(snaps)  # (cycles+1, lanes, sig)
     B.load_state(bt[0])
     B.reset_sram()
