@@ -92,8 +92,11 @@ struct PartitionOptions {
   // balanced cone size instead of chunks of target_cone, and merges keep
   // every partition's cone within the balanced bound
   uint32_t target_parts = 0;
-  // when set, merges are accepted on predicted kernel time instead of the
-  // stage-count rule
+  // balanced mode without a cost model: cut cost per distinct chunk input,
+  // in 1/16 of an AND gate (the cost model picks this weight per stage)
+  uint32_t input_weight16 = 0;
+  // when set, balanced cuts are chosen and merges accepted on predicted
+  // kernel time instead of the fixed weights and the stage-count rule
   const CostModel *cost_model = nullptr;
   const std::vector<uint8_t> *xpins = nullptr;
 };

@@ -110,16 +110,26 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
     }
   }
 
-  // ---- 2. chunking by cone size / endpoint bits
+  PackOptions po;
+  po.flat = opt.target_parts != 0;  // balanced mode targets the batched kernel
+  uint64_t cone_bound = 0;  // balanced mode: the largest chunk cost allowed
+  // Steps 2 and 3 for a balanced-cut cost of cone ANDs + SRAM weight +
+  // input_w16 / 16 per distinct chunk input (the global read of the batched
+  // kernel loads one slot per input; 0 outside balanced mode).
+  auto cut_and_pack = [&](uint64_t input_w16) {
   std::vector<std::vector<uint32_t>> chunks;
-  uint64_t cone_bound = 0;  // balanced mode: the largest chunk cone allowed
+  // ---- 2. chunking by cone size / endpoint bits
   {
     std::vector<uint32_t> mark(g.num_pins + 1, 0);
     uint32_t gen = 1;
     std::vector<uint32_t> stk;
-    // AND gates of endpoint e's cone not yet marked `gen` (marks them)
+    // AND gates of endpoint e's cone not yet marked `gen` (marks them);
+    // `leaves` receives the cone's inputs (stage inputs: staged signals,
+    // DFF / SRAM outputs, primary inputs) not yet marked
+    uint64_t leaves = 0;
     auto grow = [&](uint32_t e) {
       uint64_t add = 0;
+      leaves = 0;
       stk.clear();
       st.for_each_input(g, e, [&](uint32_t p) { stk.push_back(p); });
       while (!stk.empty()) {
@@ -127,7 +137,10 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
         stk.pop_back();
         if (mark[u] == gen) continue;
         mark[u] = gen;
-        if (st.is_leaf(g, u)) continue;
+        if (st.is_leaf(g, u)) {
+          leaves++;
+          continue;
+        }
         add++;
         stk.push_back(g.fa[u] >> 1);
         stk.push_back(g.fb[u] >> 1);
@@ -163,6 +176,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
         uint64_t add = 0;
         if (!close) {
           add = grow(e) + weight(e);
+          add += (input_w16 * leaves) >> 4;
           close = !cur.empty() && cone + add > bound;
         }
         if (close) {
@@ -172,6 +186,7 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
           cone = bits = 0;
           ++gen;
           add = grow(e) + weight(e);
+          add += (input_w16 * leaves) >> 4;
         }
         cur.push_back(e);
         cone += add;
@@ -189,7 +204,10 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
       // chunks (binary search; the whole stage as one chunk is the top)
       uint64_t lo = 1, hi = 0;
       ++gen;
-      for (uint32_t e : order) hi += grow(e) + weight(e);
+      for (uint32_t e : order) {
+        hi += grow(e) + weight(e);
+        hi += (input_w16 * leaves) >> 4;
+      }
       hi = std::max<uint64_t>(hi, 1);
       while (lo < hi) {
         const uint64_t mid = lo + (hi - lo) / 2;
@@ -225,8 +243,6 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
   }
 
   // ---- 3. pack; split failures in half
-  PackOptions po;
-  po.flat = opt.target_parts != 0;  // balanced mode targets the batched kernel
   std::vector<Partition> good;
   while (!chunks.empty()) {
     std::vector<Partition> built(chunks.size());
@@ -249,73 +265,43 @@ std::vector<Partition> partition_stage(const AIG &g, const StagedAIG &st,
     chunks.swap(retry);
   }
 
-  // ---- 3b. learned refinement (balanced mode with a cost model).  All
-  // partitions of a stage run at once, so the stage lasts as long as the
-  // slowest.  While it helps, endpoints move across a boundary of the
-  // partition predicted slowest: its first or last 1/16, 1/8 or 1/4 go to
-  // the neighbour on that side, and the move that gives the smallest larger
-  // prediction of the two is taken if that is below the old maximum.
-  if (opt.target_parts && opt.cost_model && opt.cost_model->valid() && good.size() > 1) {
-    std::vector<uint32_t> pos(ne);
-    for (size_t i = 0; i < order.size(); ++i) pos[order[i]] = (uint32_t)i;
-    std::sort(good.begin(), good.end(), [&](const Partition &a, const Partition &b) {
-      return pos[a.endpoints.front()] < pos[b.endpoints.front()];
-    });
-    auto predict = [&](const Partition &p) {
-      float f[NFEAT];
-      partition_features(g, st, p, opt.xpins, f);
-      return (double)opt.cost_model->predict(f);  // log cycles
-    };
-    std::vector<double> pred(good.size());
-    parallel_for(good.size(), threads, [&](size_t i) { pred[i] = predict(good[i]); });
-    struct Move {
-      size_t j = 0, m = 0;
-      Partition a, b;  // the slowest and its neighbour after the move
-      double worse = 0;
-      bool ok = false;
-    };
-    const size_t max_steps = 4 * good.size();
-    for (size_t step = 0; step < max_steps; ++step) {
-      const size_t i = (size_t)(std::max_element(pred.begin(), pred.end()) - pred.begin());
-      const size_t n = good[i].endpoints.size();
-      std::vector<Move> moves;
-      for (size_t j : {i - 1, i + 1}) {
-        if (j >= good.size()) continue;  // i - 1 wraps for i = 0
-        for (size_t div : {16, 8, 4}) {
-          Move mv;
-          mv.j = j;
-          mv.m = std::max<size_t>(1, n / div);
-          if (mv.m < n && (moves.empty() || moves.back().j != j || moves.back().m != mv.m))
-            moves.push_back(std::move(mv));
-        }
-      }
-      parallel_for(moves.size(), threads, [&](size_t k) {
-        Move &mv = moves[k];
-        const auto &ei = good[i].endpoints, &ej = good[mv.j].endpoints;
-        std::vector<uint32_t> ni, nj;
-        if (mv.j == i + 1) {  // i's last m lead j
-          ni.assign(ei.begin(), ei.end() - mv.m);
-          nj.assign(ei.end() - mv.m, ei.end());
-          nj.insert(nj.end(), ej.begin(), ej.end());
-        } else {  // i's first m follow j
-          ni.assign(ei.begin() + mv.m, ei.end());
-          nj = ej;
-          nj.insert(nj.end(), ei.begin(), ei.begin() + mv.m);
-        }
-        if (!build_partition(g, st, ni, mv.a, po) || !build_partition(g, st, nj, mv.b, po)) return;
-        mv.worse = std::max(predict(mv.a), predict(mv.b));
-        mv.ok = true;
+  return good;
+  };
+
+  std::vector<Partition> good;
+  if (opt.target_parts && opt.cost_model && opt.cost_model->valid()) {
+    // ---- 3b. learned choice of the cut.  All partitions of a stage run at
+    // once, so the stage lasts as long as its slowest item.  The stage is
+    // cut with several weights of chunk inputs against cone gates, and the
+    // cut whose slowest partition the cost model predicts fastest is kept
+    // (a cut with more than target_parts partitions needs a second round of
+    // items and is taken only when every cut does).
+    double best = 0;
+    size_t best_n = 0;
+    uint64_t best_bound = 0;
+    for (uint64_t w16 : {0, 4, 8, 16, 32}) {
+      std::vector<Partition> cand = cut_and_pack(w16);
+      std::vector<double> pred(cand.size());
+      parallel_for(cand.size(), threads, [&](size_t i) {
+        float f[NFEAT];
+        partition_features(g, st, cand[i], opt.xpins, f);
+        pred[i] = (double)opt.cost_model->predict(f);  // log cycles
       });
-      Move *best = nullptr;
-      for (auto &mv : moves)
-        if (mv.ok && (!best || mv.worse < best->worse)) best = &mv;
-      if (!best || best->worse >= pred[i] - 1e-3) break;
-      const size_t j = best->j;
-      good[i] = std::move(best->a);
-      good[j] = std::move(best->b);
-      pred[i] = predict(good[i]);
-      pred[j] = predict(good[j]);
+      const double worst = pred.empty() ? 0.0 : *std::max_element(pred.begin(), pred.end());
+      const size_t n = cand.size();
+      const bool over = n > opt.target_parts, best_over = best_n > opt.target_parts;
+      const bool take = good.empty() || (over != best_over ? !over
+                                         : over ? n < best_n : worst < best - 1e-6);
+      if (take) {
+        good = std::move(cand);
+        best = worst;
+        best_n = n;
+        best_bound = cone_bound;
+      }
     }
+    cone_bound = best_bound;
+  } else {
+    good = cut_and_pack(opt.target_parts ? opt.input_weight16 : 0);
   }
 
   // ---- 4. merge neighbours (in endpoint order) when it costs no stages

@@ -1689,7 +1689,54 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     // 10 bit 0 marks the form, words 11 + k the bytes of chunk k to copy
     // (header and slot words; 0 = the whole chunk).
     bool compact = all_flat && ns <= COMPACT_MAX_STAGES;
+    const uint32_t gr_top = (n_gr + 31) & ~31u;
+    // Direct variant of the compact form: a level-1 position whose b input
+    // is forced (ob) only passes its a input on, value a ^ xa and X plane
+    // a_x, so unless a hook reads it, it is not stored: its readers take its
+    // source instead, with xa folded into their own xa / xb (a ^ xa ^ xa_r
+    // and the X plane are unchanged).  Stage regions then follow the global
+    // read one after another (nothing is overwritten, so a value lives until
+    // the partition ends), which needs the global read plus every stage's
+    // stored slots to fit 8192 positions; otherwise the carries stay and the
+    // regions alternate ends of the buffer.
+    bool direct = false;
     if (compact) {
+      uint32_t total = gr_top;
+      for (uint32_t ci = 0; ci < ns; ++ci) {
+        const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
+        const uint32_t *ex = ps.ext_all[ci];
+        if (t < 8) ps.hmask[t] = 0;
+        __syncthreads();
+        for (uint32_t slot = t; slot < nio; slot += BT) {
+          const uint32_t hw = src[off + 128 + slot / 2];
+          const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+          if ((hook >> 8) == ci) atomicOr(&ps.hmask[(hook & 255u) >> 5], 1u << (hook & 31u));
+        }
+        __syncthreads();
+        uint32_t nh = 0;
+        for (int w = 0; w < 8; ++w) nh += __popc(ps.hmask[w]);
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const uint32_t pp = 4096 + 8 * t + j;
+          const bool hk = (ps.hmask[pp >> 10] >> ((pp >> 5) & 31)) & 1u;
+          const bool ob = (C[4096 + 4 * (pp >> 5) + 2] >> (pp & 31)) & 1u;
+          if (((ex[pp >> 5] >> (pp & 31)) & 1u) && !hk && !ob) ++cnt;
+        }
+        uint32_t no = 0;
+        block_excl_scan(cnt, ps.warp_sum, &no);  // ends with a barrier-free read
+        total += 32 * nh + no;
+        __syncthreads();  // hmask read by every thread before the next reset
+      }
+      direct = total <= 8192;
+    }
+    // Source references of the previous stage's positions (slot_prev) and of
+    // this stage's (slot_cur): a shared-memory word below 8192, bit 13 set
+    // when the value is to be inverted (direct variant), REF_ZERO for the
+    // constant 0 (and for positions nothing reads), REF_ONE for constant 1.
+    constexpr uint32_t REF_ZERO = 0xffffu, REF_ONE = 0xfffeu;
+    if (compact) {
+      uint32_t next_base = gr_top;
       for (uint32_t ci = 0; ci < ns; ++ci) {
         const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
         uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
@@ -1706,25 +1753,33 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         uint32_t nh = 0;
         const uint32_t bg = block_excl_scan(hooked_t ? 1u : 0u, ps.warp_sum, &nh);
         if (hooked_t) ps.blk_of[t] = (uint16_t)bg;
-        // other level-1 positions read from outside: thread t owns 4096+8t..+7
-        uint32_t mine = 0;
+        // other level-1 positions read from outside: thread t owns
+        // 4096+8t..+7; in the direct variant the pass-throughs among them are
+        // aliases (`alias`), not slots
+        uint32_t mine = 0, alias = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const uint32_t pp = 4096 + 8 * t + j;
           const bool hk = (ps.hmask[pp >> 10] >> ((pp >> 5) & 31)) & 1u;
-          if (((ex[pp >> 5] >> (pp & 31)) & 1u) && !hk) mine |= 1u << j;
+          const bool ob = (C[4096 + 4 * (pp >> 5) + 2] >> (pp & 31)) & 1u;
+          if (((ex[pp >> 5] >> (pp & 31)) & 1u) && !hk) {
+            if (direct && ob)
+              alias |= 1u << j;
+            else
+              mine |= 1u << j;
+          }
         }
         uint32_t no = 0;
         uint32_t rk = block_excl_scan(__popc(mine), ps.warp_sum, &no);
         const uint32_t n = 32 * nh + no;
-        const uint32_t base = (ci & 1) ? 0u : 8192u - n;
-        const uint32_t gr_top = (n_gr + 31) & ~31u;
-        const uint32_t ov = (ci == 0 && gr_top > base) ? gr_top - base : 0u;
+        const uint32_t base = direct ? next_base : (ci & 1) ? 0u : 8192u - n;
+        next_base += n;
+        const uint32_t ov = (!direct && ci == 0 && gr_top > base) ? gr_top - base : 0u;
         if (ov > 4 * BT) {  // stage 0 only (uniform): keep the tree form
           compact = false;
           break;
         }
-        for (uint32_t pp = t; pp < 8192; pp += BT) ps.slot_cur[pp] = 0xffffu;
+        for (uint32_t pp = t; pp < 8192; pp += BT) ps.slot_cur[pp] = (uint16_t)REF_ZERO;
         __syncthreads();
         for (uint32_t pp = t; pp < 8192; pp += BT) {
           const uint32_t g = pp >> 5;
@@ -1736,25 +1791,36 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
+          const uint32_t pp = 4096 + 8 * t + j;
           if ((mine >> j) & 1u) {
-            const uint32_t pp = 4096 + 8 * t + j, sl = 32 * nh + rk++;
+            const uint32_t sl = 32 * nh + rk++;
             ps.slot_cur[pp] = (uint16_t)(base + sl);
             ps.pos_of[sl] = (uint16_t)pp;
+          } else if ((alias >> j) & 1u) {
+            // the a input's reference, inverted once more when xa is set
+            const uint32_t xa = (C[4096 + 4 * (pp >> 5)] >> (pp & 31)) & 1u;
+            const uint32_t sa = perm_src(C, pp - 4096) & 8191u;
+            uint32_t r = (ci > 0 && sa == 0) ? REF_ZERO : ps.slot_prev[sa];
+            if (xa) r = r == REF_ZERO ? REF_ONE : r == REF_ONE ? REF_ZERO : r ^ (1u << 13);
+            ps.slot_cur[pp] = (uint16_t)r;
           }
         }
         __syncthreads();
         for (uint32_t i = t; i < n; i += BT) {
           const uint32_t P = ps.pos_of[i];
           const uint32_t *F = C + 4096 + 4 * (P >> 5);
-          const uint32_t xa = (F[0] >> (P & 31)) & 1u, xb = (F[1] >> (P & 31)) & 1u,
-                         ob = (F[2] >> (P & 31)) & 1u;
+          uint32_t xa = (F[0] >> (P & 31)) & 1u, xb = (F[1] >> (P & 31)) & 1u;
+          const uint32_t ob = (F[2] >> (P & 31)) & 1u;
           const uint32_t sa = perm_src(C, P - 4096) & 8191u, sb = perm_src(C, P) & 8191u;
           // a source of stage >= 1 at position 0 is the constant 0
-          const uint32_t wa = (ci > 0 && sa == 0) ? 0xffffu : ps.slot_prev[sa];
-          const uint32_t wb = (ob || (ci > 0 && sb == 0)) ? 0xffffu : ps.slot_prev[sb];
-          const uint32_t za = wa == 0xffffu, zb = wb == 0xffffu;
-          D[4 + i] = (za ? 0u : wa) | ((zb ? 0u : wb) << 13) | (xa << 26) | (xb << 27) | (ob << 28) |
-                 (za << 29) | (zb << 30);
+          const uint32_t ra = (ci > 0 && sa == 0) ? REF_ZERO : ps.slot_prev[sa];
+          const uint32_t rb = (ob || (ci > 0 && sb == 0)) ? REF_ZERO : ps.slot_prev[sb];
+          const uint32_t za = ra >= REF_ONE, zb = rb >= REF_ONE;
+          // an inverted source (or the constant 1) flips the input's own flag
+          xa ^= za ? (ra == REF_ONE) : (ra >> 13) & 1u;
+          xb ^= zb ? (rb == REF_ONE) : (rb >> 13) & 1u;
+          const uint32_t wa = za ? 0u : ra & 8191u, wb = zb ? 0u : rb & 8191u;
+          D[4 + i] = wa | (wb << 13) | (xa << 26) | (xb << 27) | (ob << 28) | (za << 29) | (zb << 30);
         }
         if (t == 0) {
           D[0] = n;
