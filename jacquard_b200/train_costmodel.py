@@ -11,10 +11,12 @@
    out the grid-barrier wait) and records log(mean SM cycles per work item)
    next to the partition's 24 features.
 3. Trains the MLP with Adam (lr 1e-3, batch 512) on the GPU kernels.
-4. Evaluates on a fresh design: balanced partitions without and with the
-   learned refinement (the partitioner moves endpoints off the partition
-   predicted slowest in each stage), device-timed stimulus-cycles/s of the
-   batched interpreter, same stimulus.
+4. Evaluates on fresh designs: balanced partitions without and with the
+   learned cut choice (each major stage is cut with several weights of a
+   chunk's inputs against its gates, and the cut whose slowest partition
+   the model predicts fastest is kept), device-timed stimulus-cycles/s of
+   the batched interpreter on the same random stimulus, and every DFF and
+   output value of both runs compared bit for bit.
 """
 import argparse
 import json
@@ -24,7 +26,7 @@ import time
 import numpy as np
 import torch
 
-from . import batched, costmodel, frontend
+from . import batched, costmodel, frontend, state
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -74,36 +76,75 @@ def collect(target, seed0=100, log=print):
     return np.concatenate(feats)[:target], np.concatenate(ys)[:target]
 
 
+def _lane_stimulus(script, design, lanes, cycles, seed):
+    """(cycles+1, lanes, input signals) lane words: every primary input of
+    every stream toggles with probability 1/4 per cycle, the clock flag is 1,
+    the reset input is 1 for the first 4 snapshots."""
+    rng = np.random.default_rng(seed)
+    lay = np.asarray(script.input_layout)
+    pos = state.input_positions(script)
+    n = lay.size
+    w = np.empty((cycles + 1, n, lanes), np.uint32)
+    cur = rng.integers(0, 2**32, size=(n, lanes), dtype=np.uint32)
+    clk = lay == design.clock_flag_pin
+    rst = (lay == design.reset_pin) if design.reset_pin else np.zeros(n, bool)
+    for c in range(cycles + 1):
+        if c:
+            cur ^= (rng.integers(0, 2**32, size=(n, lanes), dtype=np.uint32)
+                    & rng.integers(0, 2**32, size=(n, lanes), dtype=np.uint32))
+        v = cur.copy()
+        v[clk] = 0xFFFFFFFF
+        v[rst] = 0xFFFFFFFF if c < 4 else 0
+        w[c] = v
+    rows = np.zeros((cycles + 1, lanes, batched.input_words(script) * 32), np.uint32)
+    rows[:, :, pos] = np.swapaxes(w, 1, 2)
+    return rows
+
+
 def evaluate(model_packed, clusters=1024, cycles=5000, lanes=8, seed=4242, split=4, parts=74,
              log=print):
-    """Balanced partitions without and with the learned refinement on one
+    """Balanced partitions without and with the learned cut choice on one
     fresh design: batched stimulus-cycles/s over `cycles` cycles (device
-    time, one launch each).  74 partitions per stage make two rounds of
-    lane-pair items on 148 CTAs (37 leave partitions too large to pack)."""
+    time, one launch each), same random stimulus.  Both runs must end with
+    the same value in every DFF and primary output of every stream (their
+    state layouts differ, the netlist does not): the learned run is checked
+    bit for bit against the heuristic one."""
     d = frontend.Design(frontend.soc_params(seed=seed, n_clusters=clusters,
                                             n_dff=200_000 * clusters // 512))
     out = {"design_ands": int(d.num_and), "cycles": cycles, "streams": 32 * lanes,
            "split": split, "parts_per_stage": parts}
+    finals = {}
     for name, cm in (("heuristic", None), ("learned", model_packed)):
         t0 = time.perf_counter()
         s = build(d, split, parts, cost_model=cm)
         bt = time.perf_counter() - t0
         B = batched.BatchedSim(s, lanes)
-        B.load_state(np.zeros((lanes, B.sig), np.uint32))
-        B.reset_sram()
-        B.run(None, 2)
+        rows = _lane_stimulus(s, d, lanes, cycles, seed + 1)
+        snap0 = np.zeros((lanes, B.sig), np.uint32)
+        snap0[:, :B.in_sigs] = rows[0]
+        B.load_state(snap0)
+        B.reset_sram(x=False)
+        stim = torch.from_numpy(np.ascontiguousarray(rows).reshape(-1).view(np.int32)).cuda()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        B.run(None, cycles)
+        B.run(stim, cycles)
         e1.record()
         torch.cuda.synchronize()
         assert B.status() == 0
         ms = e0.elapsed_time(e1)
-        out[name] = {"stream_cycles_per_s": 32 * lanes * cycles / (ms / 1e3), "partitions": s.num_partitions,
+        fin = B.final_state(cycles).cpu().numpy().view(np.uint32).reshape(lanes, B.sig)
+        dq = state.dff_positions(s, d)
+        po = state.po_positions(s, d)
+        finals[name] = (fin[:, dq], fin[:, po])  # lane words: value of each DFF / output
+        out[name] = {"stream_cycles_per_s": 32 * lanes * cycles / (ms / 1e3),
+                     "partitions": s.num_partitions,
                      "script_mb_per_cycle": s.script_words_per_cycle() * 4 / 1e6, "build_s": bt}
         log(f"  {name}: {out[name]}")
+    out["bit_exact_vs_heuristic"] = bool(
+        np.array_equal(finals["heuristic"][0], finals["learned"][0])
+        and np.array_equal(finals["heuristic"][1], finals["learned"][1]))
     out["gain"] = out["learned"]["stream_cycles_per_s"] / out["heuristic"]["stream_cycles_per_s"]
     return out
 
@@ -116,7 +157,16 @@ def main():
     ap.add_argument("--eval-clusters", type=int, default=1024)
     ap.add_argument("--eval-cycles", type=int, default=5000)
     ap.add_argument("--eval-parts", type=int, default=74, help="partitions per major stage")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="evaluate the model saved at --out (no collection or training)")
     args = ap.parse_args()
+    if args.eval_only:
+        packed = costmodel.packed_from_file(args.out)
+        ev = evaluate(packed, clusters=args.eval_clusters, cycles=args.eval_cycles,
+                      parts=args.eval_parts)
+        ev_soc = evaluate(packed, clusters=512, cycles=args.eval_cycles, seed=2, parts=37)
+        print(json.dumps({"eval": ev, "eval_soc2m": ev_soc}))
+        return
     t0 = time.time()
     X, y = collect(args.samples)
     print(f"collected {len(y)} partitions in {time.time() - t0:.0f}s; log-cycles mean {y.mean():.2f} sd {y.std():.2f}")
