@@ -4,14 +4,17 @@ single-port 1024x32 SRAMs, 128 PIs, X-propagation on, all DFF/SRAM state X at
 start, 16 reset cycles then p_toggle = 0.25 stimulus).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
-                  [--mode plain|batched] [--lanes L] [--window C] [--learned]
+                  [--mode batched|timed|plain|timed_plain|multi] [--lanes L]
+                  [--window C] [--learned auto|on|off] [--no-check]
 
 One step = one launch window of C cycles over all stimulus streams.  The
 batched mode partitions every major stage into blocks / (lanes / 2) balanced
-partitions (one round of lane-pair work items); --learned adds the cost
-model's refinement of that cut.  `value`
-is device-timed throughput with inputs resident in HBM; `e2e` is the same
-through the C ABI with host buffers copied in and out inside the timed region.
+partitions (one round of lane-pair work items); with --learned the cost model
+chooses each stage's cut (auto: only when the committed training summary
+shows it winning, bit-exact, on this design).  `value` is device-timed
+throughput with inputs resident in HBM; `e2e` is the same through the C ABI
+with host buffers copied in and out inside the timed region; `parity` is the
+replay of two sampled streams of both timed regions on the plain interpreter.
 --impl reference runs the reference's CPU interpreter path (this repository's
 C restatement of it, oracle/) on the host cores.  Multi-GPU: independent
 replicas (one design + its own stimulus streams per rank), weak scaling.
@@ -196,6 +199,20 @@ def learned_model():
         return None
     from jacquard_b200 import costmodel
     return costmodel.packed_from_file(MODEL_PATH)
+
+
+def learned_wins():
+    """Whether the committed training summary shows the learned cut beating
+    the heuristic on this workload's own design (the 2M-gate SoC, 37
+    partitions per stage, 256 streams), with the learned run bit-exact
+    against the heuristic one.  The benchmark uses the learned cut by
+    default only then."""
+    p = os.path.splitext(MODEL_PATH)[0] + ".json"
+    if not os.path.exists(MODEL_PATH) or not os.path.exists(p):
+        return False
+    with open(p) as f:
+        ev = json.load(f).get("eval_soc2m", {})
+    return bool(ev.get("bit_exact_vs_heuristic")) and ev.get("gain", 0.0) > 1.0
 
 
 def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0):
@@ -420,7 +437,8 @@ def run_mine_batched(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
-    model = learned_model() if args.learned else None
+    use_learned = args.learned == "on" or (args.learned == "auto" and learned_wins())
+    model = learned_model() if use_learned else None
     s = build_script(d, args.blocks, cost_model=model,
                      target_parts=args.blocks // max(1, args.lanes // 2))
     lanes = args.lanes
@@ -492,7 +510,8 @@ def run_mine_batched(args, rank, world):
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
                             partitioner="balanced: at most %d per major stage%s"
                             % (args.blocks // max(1, args.lanes // 2),
-                               ", learned refinement" if model is not None else "")),
+                               ", cut chosen by the learned cost model" if model is not None
+                               else ", heuristic cut")),
                 script=s, d=d)
 
 
@@ -827,8 +846,9 @@ def main():
     ap.add_argument("--clusters", type=int, default=512,
                     help="design size in 4096-gate clusters (512 = the 2M-gate workload)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--learned", action="store_true",
-                    help="batched: the learned cost model refines the balanced partitions")
+    ap.add_argument("--learned", default="auto", choices=["auto", "on", "off"],
+                    help="batched / timed: the learned cost model chooses each stage's balanced "
+                         "cut (auto: when its recorded gain on this design is above 1)")
     ap.add_argument("--no-check", action="store_true",
                     help="batched: skip the bit-exactness self-check of the timed windows")
     ap.add_argument("--compare", action="store_true",

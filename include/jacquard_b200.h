@@ -101,6 +101,11 @@ typedef struct {
   uint32_t first_cycle; /* cycle number reported in events */
   uint64_t barrier_timeout_cycles; /* 0 = default (about a second) */
   void *stream; /* cudaStream_t, NULL = legacy default stream */
+  /* Optional stage-depth tables from jq_plain_prepare (both or neither,
+   * device): levels of a boomerang stage whose outputs nothing reads are
+   * skipped.  NULL runs every level. */
+  const uint8_t *stage_depth;
+  const uint32_t *stage_depth_base;
 } jq_sim_args;
 
 /* Barrier slots.  Each interpreter (plain, batched) keeps its grid-barrier
@@ -123,6 +128,22 @@ int jq_simulate(const jq_sim_args *a);
  * JQ_ERR_CUDA for the plain launches made so far on it, and clears the
  * recorded error. */
 int jq_sim_status(void *stream);
+
+/* Stage depth of a script for the plain interpreter (no counterpart in the
+ * reference): for every boomerang stage, the deepest tree level whose
+ * outputs a writeout hook or a needed gather of the next stage reads
+ * (0: only the first AND level, positions 4096..8191; 1: nothing below
+ * position 512; 2: any).  stage_depth_base (device, num_blocks *
+ * num_major_stages words) receives each (major stage, block) entry's first
+ * code; stage_depth (device, depth_capacity bytes) the codes, partitions in
+ * script order.  With stage_depth NULL only *num_stages (the size needed) is
+ * computed.  JQ_ERR_INVALID_ARG when depth_capacity is too small.
+ * Synchronizes `stream`.  The legacy wrappers compute these tables on every
+ * call into a device buffer the library keeps per device (allocated on the
+ * first call, grown for larger scripts). */
+int jq_plain_prepare(const size_t *blocks_start, const uint32_t *blocks_data, size_t num_blocks,
+                     size_t num_major_stages, uint32_t *stage_depth_base, uint8_t *stage_depth,
+                     size_t depth_capacity, size_t *num_stages, void *stream);
 
 /* Largest grid the plain interpreter can keep co-resident on `device`. */
 int jq_max_blocks(int device, size_t *max_blocks);

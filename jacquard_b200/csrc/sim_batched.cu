@@ -43,6 +43,11 @@ constexpr uint32_t CHUNK_BYTES = STAGE_WORDS * 4;
 // monotonic within a launch (never reset between major stages).
 static __device__ unsigned long long g_bcount[BAR_SLOTS];
 static __device__ unsigned long long g_bticket[BAR_SLOTS];
+// Arrival counts of lane-pair groups (see jq_batched_kernel): lane pairs
+// never read each other's words, so when every CTA runs one item of a fixed
+// lane pair, the CTAs of a lane pair synchronize only among themselves.
+constexpr uint32_t MAX_GROUPS = 16;
+static __device__ unsigned long long g_bgroup[BAR_SLOTS * MAX_GROUPS];
 
 __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
   unsigned long long v;
@@ -213,6 +218,8 @@ struct Shared {
   uint32_t st_nio[MAX_MAJOR_STAGES];
   uint32_t st_io[MAX_MAJOR_STAGES];
   size_t script_words;  // blocks_start[num_major_stages * num_blocks]
+  unsigned long long *bar_count;  // this CTA's grid-barrier arrival count
+  uint32_t bar_size;              // CTAs that arrive on it per barrier
 };
 
 // Bytes to copy of chunk k of a partition: compact partitions list the
@@ -235,11 +242,11 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
   asm volatile("prefetch.L2 [%0];" ::"l"(p));
 }
 
-__device__ __forceinline__ void grid_arrive(const BatchParams &P, unsigned long long &bar_target) {
+__device__ __forceinline__ void grid_arrive(const Shared &sh, unsigned long long &bar_target) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    bar_target += gridDim.x;
-    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(&g_bcount[P.slot]) : "memory");
+    bar_target += sh.bar_size;
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(sh.bar_count) : "memory");
   }
 }
 
@@ -251,7 +258,7 @@ __device__ bool grid_wait(const BatchParams &P, Shared &sh, unsigned long long b
   if (t == 0) {
     int ok = 1;
     uint64_t t0 = clock64();
-    while (ld_acquire64(&g_bcount[P.slot]) < bar_target) {
+    while (ld_acquire64(sh.bar_count) < bar_target) {
       if (*((volatile int *)&g_status[P.slot]) != 0) {
         ok = 0;
         break;
@@ -1299,6 +1306,23 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
     sh.st_io[t] = io;
   }
   __syncthreads();
+  // Lane-pair groups: with lane pairs and one item per CTA in every major
+  // stage, CTA i always runs lane pair i % per, and the CTAs of one lane
+  // pair (which alone read and write that pair's state words, SRAM rows,
+  // stimulus and outputs) form their own barrier group.
+  const uint32_t per_lp = P.lanes / NL;
+  bool grouped = NL == 2 && per_lp > 1 && per_lp <= MAX_GROUPS && gridDim.x >= per_lp;
+  for (unsigned ms = 0; ms < P.num_major_stages; ++ms) grouped &= sh.st_items[ms] <= gridDim.x;
+  const uint32_t grp = grouped ? blockIdx.x % per_lp : 0;         // lane pair of this CTA
+  const uint32_t grp_rank = grouped ? blockIdx.x / per_lp : blockIdx.x;
+  const uint32_t grp_ctas = grouped ? (gridDim.x - grp + per_lp - 1) / per_lp : gridDim.x;
+  if (t == 0) {
+    sh.bar_count = grouped ? &g_bgroup[(size_t)P.slot * MAX_GROUPS + grp] : &g_bcount[P.slot];
+    sh.bar_size = grp_ctas;
+  }
+  // lanes this CTA copies stimulus for and records: its lane pair, or all
+  const uint32_t lane_lo = grouped ? 2 * grp : 0, lane_n = grouped ? 2 : P.lanes;
+  __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
   // thread 0: arrival count that completes the next grid barrier, and the
@@ -1320,9 +1344,9 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       // stimulus signals [src, src+count) to state signals [dst, dst+count)
       // (one region at 0 when no list is given)
       const uint32_t *src = P.stim + (c + 1) * P.input_sigs * P.lanes;
-      for (size_t q = (size_t)blockIdx.x * BT + t; q < P.input_sigs * P.lanes;
-           q += (size_t)gridDim.x * BT) {
-        const size_t l = q / P.input_sigs, i = q % P.input_sigs;
+      for (size_t q = (size_t)grp_rank * BT + t; q < P.input_sigs * lane_n;
+           q += (size_t)grp_ctas * BT) {
+        const size_t l = lane_lo + q / P.input_sigs, i = q % P.input_sigs;
         size_t dst = i;
         if (P.input_regions) {
           for (uint32_t r = 0; r < P.n_input_regions; ++r) {
@@ -1331,7 +1355,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
             if (i >= s0 && i < s0 + n) dst = d0 + (i - s0);
           }
         }
-        out[phys(P, (uint32_t)l, dst)] = src[q];
+        out[phys(P, (uint32_t)l, dst)] = src[l * P.input_sigs + i];
       }
     }
     for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
@@ -1401,7 +1425,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       // every CTA takes exactly one ticket past the last item of a dynamic
       // stage, so the next stage's tickets start items + grid on
       if (t == 0 && dyn) ticket_base += items + gridDim.x;
-      grid_arrive(P, bar_target);
+      grid_arrive(sh, bar_target);
       if (DEFER && ms + 1 < P.num_major_stages) {
         pending = true;  // the wait comes with the next item
       } else {
@@ -1423,15 +1447,16 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
       }
     }
     // record outputs of this cycle
-    for (size_t q = (size_t)blockIdx.x * BT + t; q < (size_t)P.n_po * P.lanes;
-         q += (size_t)gridDim.x * BT) {
-      const uint32_t po = (uint32_t)(q / P.lanes), l = (uint32_t)(q % P.lanes);
+    for (size_t q = (size_t)grp_rank * BT + t; q < (size_t)P.n_po * lane_n;
+         q += (size_t)grp_ctas * BT) {
+      const uint32_t po = (uint32_t)(q / lane_n), l = lane_lo + (uint32_t)(q % lane_n);
       P.wave[(c * P.n_po + po) * P.lanes + l] = ldcg(out + phys(P, l, P.po_sig[po]));
     }
     if (P.record) {  // lane-major [lane][signal]
-      uint32_t *dst = P.record + (c + 1) * snap;
-      for (size_t q = (size_t)blockIdx.x * BT + t; q < snap; q += (size_t)gridDim.x * BT)
-        dst[q] = ldcg(out + phys(P, (uint32_t)(q / P.sig_per_snap), q % P.sig_per_snap));
+      uint32_t *dst = P.record + (c + 1) * snap + (size_t)lane_lo * P.sig_per_snap;
+      for (size_t q = (size_t)grp_rank * BT + t; q < P.sig_per_snap * lane_n;
+           q += (size_t)grp_ctas * BT)
+        dst[q] = ldcg(out + phys(P, lane_lo + (uint32_t)(q / P.sig_per_snap), q % P.sig_per_snap));
     }
     // the recording reads `out`; the next cycle writes into `in`: the next
     // major-stage barrier already orders them, no extra barrier needed.
@@ -1905,6 +1930,7 @@ __global__ void jq_batched_reset_kernel(int slot) {
   g_bcount[slot] = 0;
   g_bticket[slot] = 0;
   g_status[slot] = 0;
+  for (uint32_t g = 0; g < MAX_GROUPS; ++g) g_bgroup[(size_t)slot * MAX_GROUPS + g] = 0;
 }
 
 extern "C" {

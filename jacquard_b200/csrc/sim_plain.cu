@@ -10,6 +10,15 @@
 // Script chunks are streamed with 16-byte read-only loads, double-buffered in
 // registers one stage ahead.  State/SRAM reads bypass L1 (written by other
 // SMs between barriers).
+//
+// Stage depth.  An optional table (jq_plain_prepare) gives, per boomerang
+// stage of every partition, the deepest tree level whose outputs anything
+// reads (a writeout hook or a needed gather of the next stage): 0 when only
+// the first AND level (positions 4096..8191) is read, 1 when nothing below
+// position 512 is, 2 otherwise.  Levels whose outputs nobody reads are
+// skipped with their CTA barriers; the values that are read are computed as
+// before.  The shuffled inputs go to their own buffer (s_in), so a stage
+// needs one barrier before its first AND level instead of two.
 #include "sim_common.cuh"
 
 namespace jqk {
@@ -28,6 +37,8 @@ struct PlainParams {
   uint32_t first_cycle;
   uint64_t timeout;
   int slot;
+  const uint8_t *depth;         // stage depth codes, or null (every level runs)
+  const uint32_t *depth_base;   // first code of each (major stage, block) entry
 };
 
 template <bool TRACK>
@@ -35,7 +46,8 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
                                           const uint32_t *in, uint32_t *out, uint32_t cycle,
                                           uint32_t *s_meta, uint32_t *s_st, uint32_t *s_stx,
                                           uint32_t *s_wo, uint32_t *s_wox, uint16_t *s_arr,
-                                          uint16_t *s_woarr) {
+                                          uint16_t *s_woarr, uint32_t *s_in, uint32_t *s_inx,
+                                          const uint8_t *depth) {
   const int t = threadIdx.x;
   const uint32_t clock_ps = TRACK && P.constraints ? __ldg(P.constraints) : 0;
   const uint32_t *cons = P.constraints ? P.constraints + 1 : nullptr;
@@ -84,6 +96,7 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
     // ---- boomerang stages
     for (uint32_t bs = 0; bs < ns; ++bs) {
       const uint32_t *nx = ch + STAGE_WORDS * (bs + 1);
+      const uint32_t dcode = depth ? depth[bs] : 2u;
       uint32_t hin = gather16(s_st, c0, c1, c2, c3);
       uint32_t hinx = is_x ? gather16(s_stx, c0, c1, c2, c3) : 0u;
       const uint32_t xa = cf.x, xb = cf.y, ob = cf.z;
@@ -94,22 +107,26 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
       c2 = ldg4(nx + 2048 + 4 * t);
       c3 = ldg4(nx + 3072 + 4 * t);
       cf = ldg4(nx + 4096 + 4 * t);
-      __syncthreads();
-      s_st[t] = hin;
-      s_stx[t] = hinx;
-      __syncthreads();
-      // level 0: threads 128..255; inputs' arrivals are 0 after the shuffle
+      s_in[t] = hin;
+      s_inx[t] = hinx;
+      __syncthreads();  // every gather from s_st done, every input word in s_in
+      // level 0: threads 128..255; inputs' arrivals are 0 after the shuffle.
+      // Threads below 128 keep their input word at their position: the
+      // deeper levels never read it (they read level-0 outputs upwards).
       if (t >= 128) {
         uint32_t r, rx;
-        xand(s_st[t - 128], s_stx[t - 128], hin, hinx, xa, xb, ob, r, rx);
+        xand(s_in[t - 128], s_inx[t - 128], hin, hinx, xa, xb, ob, r, rx);
         s_st[t] = r;
         if (is_x) s_stx[t] = rx;
         if (TRACK) s_arr[t] = dly;
-      } else if (TRACK) {
-        s_arr[t] = 0;
+      } else {
+        s_st[t] = hin;
+        s_stx[t] = hinx;
+        if (TRACK) s_arr[t] = 0;
       }
       __syncthreads();
       // levels 1..3 in shared memory
+      if (dcode >= 1) {
 #pragma unroll
       for (int hi = 1; hi <= 3; ++hi) {
         const int w = 1 << (7 - hi);
@@ -122,7 +139,9 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
         }
         __syncthreads();
       }
+      }
       // levels 4..7 inside warp 0, levels 8..12 bit-level in thread 0
+      if (dcode >= 2) {
       if (t < 32) {
         uint32_t cur = s_st[t], curx = s_stx[t];
         uint32_t ca = TRACK ? (uint32_t)s_arr[t] : 0u;
@@ -176,6 +195,7 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
         if (TRACK) s_arr[t] = (uint16_t)ca;
       }
       __syncthreads();
+      }
       if ((hook >> 8) == bs) {
         const uint32_t src = hook & 255u;
         s_wo[t] = s_st[src];
@@ -256,6 +276,7 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
       }
     }
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    if (depth) depth += ns;
     if (is_last) break;
     __syncthreads();
   }
@@ -263,7 +284,7 @@ __device__ __forceinline__ void run_block(const PlainParams &P, const uint32_t *
 
 template <bool TRACK>
 __global__ void __launch_bounds__(NT, 3) jq_plain_kernel(PlainParams P) {
-  __shared__ uint32_t s_meta[NT], s_st[NT], s_stx[NT], s_wo[NT], s_wox[NT];
+  __shared__ uint32_t s_meta[NT], s_st[NT], s_stx[NT], s_wo[NT], s_wox[NT], s_in[NT], s_inx[NT];
   __shared__ uint16_t s_arr[NT], s_woarr[NT];
   __shared__ size_t s_start[32];
   const int t = threadIdx.x;
@@ -278,10 +299,121 @@ __global__ void __launch_bounds__(NT, 3) jq_plain_kernel(PlainParams P) {
     const uint32_t *in = P.states + c * P.state_size;
     uint32_t *out = P.states + (c + 1) * P.state_size;
     for (unsigned ms = 0; ms < P.num_major_stages; ++ms) {
+      const uint8_t *dp =
+          P.depth ? P.depth + P.depth_base[(size_t)ms * P.num_blocks + blockIdx.x] : nullptr;
       run_block<TRACK>(P, P.blocks_data + s_start[ms], in, out, P.first_cycle + (uint32_t)c,
-                       s_meta, s_st, s_stx, s_wo, s_wox, s_arr, s_woarr);
+                       s_meta, s_st, s_stx, s_wo, s_wox, s_arr, s_woarr, s_in, s_inx, dp);
       if (!grid_barrier(P.slot, P.num_blocks, P.timeout)) return;
     }
+  }
+}
+
+// 16-bit shuffle index q (0..8191) of a boomerang chunk: bit k of thread T
+// at chunk[(k>>3)*1024 + T*4 + ((k>>1)&3)], low half for even k
+// (src/flatten.rs:984-1076).
+__device__ __forceinline__ uint32_t shuffle_src(const uint32_t *chunk, uint32_t q) {
+  const uint32_t T = q >> 5, k = q & 31;
+  const uint32_t w = chunk[(k >> 3) * 1024 + T * 4 + ((k >> 1) & 3)];
+  return ((k & 1) ? (w >> 16) : (w & 0xffffu)) & 8191u;
+}
+
+// Boomerang stages per (major stage, block) entry.
+__global__ void jq_plain_stage_count_kernel(const size_t *blocks_start, const uint32_t *script,
+                                            uint32_t *counts, unsigned entries) {
+  const unsigned e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= entries) return;
+  size_t off = blocks_start[e];
+  uint32_t n = 0;
+  for (;;) {
+    const uint32_t ns = script[off];
+    if (!ns) break;
+    n += ns;
+    if (script[off + 1]) break;
+    off += 256 + 512 * (size_t)script[off + 6] + STAGE_WORDS * ((size_t)ns + 2);
+  }
+  counts[e] = n;
+}
+
+// Stage depth codes of one (major stage, block) entry's partitions (one CTA
+// of NT threads per entry).  Walking each partition's stages last to first:
+// a tree position is read from outside its stage when a writeout hook of the
+// stage covers its word or a needed gather of the next stage names it, and
+// it is live when it is read from outside or its parent is live (children
+// [2L, 3L) are the a inputs of [L, 2L), [3L, 4L) its b inputs).  A gather of
+// a first-level position (4096..8191) is needed when the position is live,
+// except the b input when ob forces it to one.  The code is 2 when a
+// position below 512 is live, else 1 when one below 4096 is, else 0.
+__global__ void __launch_bounds__(NT) jq_plain_depth_kernel(const size_t *blocks_start,
+                                                            const uint32_t *script,
+                                                            const uint32_t *depth_base,
+                                                            uint8_t *depth, unsigned entries) {
+  __shared__ uint32_t need[256], ext[256];
+  __shared__ uint8_t live[8192];
+  __shared__ int any_deep, any_mid;
+  const unsigned e = blockIdx.x;
+  if (e >= entries) return;
+  const uint32_t t = threadIdx.x;
+  size_t off = blocks_start[e];
+  uint8_t *dp = depth + depth_base[e];
+  for (;;) {
+    const uint32_t ns = script[off];
+    if (!ns) break;
+    const uint32_t nio = script[off + 2], R = script[off + 6];
+    const uint32_t *ch = script + off + 256 + 512 * (size_t)R;
+    need[t] = 0;  // nothing reads the last stage but its hooks
+    __syncthreads();
+    for (int ci = (int)ns - 1; ci >= 0; --ci) {
+      const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
+      ext[t] = need[t];
+      if (t == 0) any_deep = any_mid = 0;
+      __syncthreads();
+      for (uint32_t slot = t; slot < nio; slot += NT) {
+        const uint32_t hw = script[off + 128 + slot / 2];
+        const uint32_t hook = (slot & 1) ? (hw >> 16) : (hw & 0xffffu);
+        if ((hook >> 8) == (uint32_t)ci) ext[hook & 255u] = 0xffffffffu;
+      }
+      __syncthreads();
+      // top-down, one level per pass: position 1, then [2, 4), ..., [4096, 8192)
+      if (t == 0) live[0] = 0;
+      for (uint32_t M = 1; M <= 4096; M <<= 1) {
+        for (uint32_t c = M + t; c < 2 * M; c += NT) {
+          uint8_t l = (uint8_t)((ext[c >> 5] >> (c & 31)) & 1u);
+          if (M > 1) {
+            const uint32_t h = M >> 1;
+            l |= live[c < M + h ? c - h : c - M];
+          }
+          live[c] = l;
+        }
+        __syncthreads();
+      }
+      int deep = 0, mid = 0;
+      for (uint32_t c = 1 + t; c < 4096; c += NT) {
+        if (live[c]) {
+          if (c < 512) deep = 1;
+          else mid = 1;
+        }
+      }
+      if (deep) any_deep = 1;
+      if (mid) any_mid = 1;
+      need[t] = 0;
+      __syncthreads();
+      // the previous stage's positions that this stage's needed gathers read
+      for (uint32_t P = 4096 + t; P < 8192; P += NT) {
+        if (!live[P]) continue;
+        const uint32_t sa = shuffle_src(C, P - 4096);
+        atomicOr(&need[sa >> 5], 1u << (sa & 31));
+        const bool ob = (C[4096 + 4 * (P >> 5) + 2] >> (P & 31)) & 1u;
+        if (!ob) {
+          const uint32_t sb = shuffle_src(C, P);
+          atomicOr(&need[sb >> 5], 1u << (sb & 31));
+        }
+      }
+      if (t == 0) dp[ci] = any_deep ? 2 : any_mid ? 1 : 0;
+      __syncthreads();
+    }
+    dp += ns;
+    if (script[off + 1]) break;
+    off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
   }
 }
 
@@ -303,6 +435,93 @@ __global__ void jq_plain_reset_kernel(int slot) {
 }
 
 int g_max_blocks_cache[64];
+
+// Stage-depth tables of the legacy wrappers, per device: allocated on the
+// first call and grown when a larger script comes (the reference's wrappers
+// take no workspace), refilled by every call.
+struct DepthCache {
+  uint8_t *depth = nullptr;
+  uint32_t *base = nullptr;
+  size_t depth_cap = 0, base_cap = 0;
+};
+DepthCache g_depth_cache[64];
+
+int plain_prepare(const size_t *blocks_start, const uint32_t *blocks_data, size_t num_blocks,
+                  size_t num_major_stages, uint32_t *depth_base, uint8_t *depth,
+                  size_t depth_capacity, size_t *num_stages, cudaStream_t st) {
+  const size_t entries = num_blocks * num_major_stages;
+  jq_plain_stage_count_kernel<<<(unsigned)((entries + 255) / 256), 256, 0, st>>>(
+      blocks_start, blocks_data, depth_base, (unsigned)entries);
+  if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
+  uint32_t *h = (uint32_t *)malloc(entries * sizeof(uint32_t));
+  if (!h) return JQ_ERR_INVALID_ARG;
+  int rc = JQ_OK;
+  if (cudaMemcpyAsync(h, depth_base, entries * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    rc = JQ_ERR_CUDA;
+  } else {
+    size_t total = 0;
+    for (size_t e = 0; e < entries; ++e) {
+      const uint32_t c = h[e];
+      h[e] = (uint32_t)total;
+      total += c;
+    }
+    if (num_stages) *num_stages = total;
+    if (!depth) {
+      // counting only
+    } else if (total > depth_capacity || total > 0xffffffffu) {
+      rc = JQ_ERR_INVALID_ARG;
+    } else {
+      if (cudaMemcpyAsync(depth_base, h, entries * sizeof(uint32_t), cudaMemcpyHostToDevice, st) !=
+          cudaSuccess) {
+        rc = JQ_ERR_CUDA;
+      } else {
+        jq_plain_depth_kernel<<<(unsigned)entries, NT, 0, st>>>(blocks_start, blocks_data,
+                                                                depth_base, depth,
+                                                                (unsigned)entries);
+        if (cudaGetLastError() != cudaSuccess) rc = JQ_ERR_LAUNCH;
+        else if (cudaStreamSynchronize(st) != cudaSuccess) rc = JQ_ERR_CUDA;
+      }
+    }
+  }
+  free(h);
+  return rc;
+}
+
+// The legacy wrappers' stage-depth tables for this script (device memory
+// of the cache); false when they cannot be made, and then every level runs.
+bool legacy_depth(jq_sim_args *a) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  DepthCache &dc = g_depth_cache[dev];
+  const size_t entries = a->num_blocks * a->num_major_stages;
+  if (dc.base_cap < entries) {
+    if (dc.base) cudaFree(dc.base);
+    dc.base = nullptr;
+    dc.base_cap = 0;
+    if (cudaMalloc(&dc.base, entries * sizeof(uint32_t)) != cudaSuccess) return false;
+    dc.base_cap = entries;
+  }
+  size_t stages = 0;
+  if (plain_prepare(a->blocks_start, a->blocks_data, a->num_blocks, a->num_major_stages, dc.base,
+                    nullptr, 0, &stages, nullptr) != JQ_OK ||
+      stages == 0)
+    return false;
+  if (dc.depth_cap < stages) {
+    if (dc.depth) cudaFree(dc.depth);
+    dc.depth = nullptr;
+    dc.depth_cap = 0;
+    if (cudaMalloc(&dc.depth, stages) != cudaSuccess) return false;
+    dc.depth_cap = stages;
+  }
+  if (plain_prepare(a->blocks_start, a->blocks_data, a->num_blocks, a->num_major_stages, dc.base,
+                    dc.depth, dc.depth_cap, nullptr, nullptr) != JQ_OK)
+    return false;
+  a->stage_depth = dc.depth;
+  a->stage_depth_base = dc.base;
+  return true;
+}
 
 int launch_plain(const jq_sim_args *a, uint32_t event_cap) {
   if (!a || a->num_blocks == 0 || a->num_major_stages == 0 || a->num_major_stages > 32 ||
@@ -335,6 +554,9 @@ int launch_plain(const jq_sim_args *a, uint32_t event_cap) {
   P.first_cycle = a->first_cycle;
   P.timeout = a->barrier_timeout_cycles ? a->barrier_timeout_cycles : DEFAULT_BARRIER_TIMEOUT;
   P.slot = slot;
+  P.depth = a->stage_depth;
+  P.depth_base = a->stage_depth_base;
+  if ((P.depth == nullptr) != (P.depth_base == nullptr)) return JQ_ERR_INVALID_ARG;
   // reset this slot's barrier (ordered before the kernel on the stream)
   jq_plain_reset_kernel<<<1, 1, 0, st>>>(slot);
   if (cudaGetLastError() != cudaSuccess) return JQ_ERR_LAUNCH;
@@ -375,7 +597,10 @@ int read_status(void *stream) {
 // ended that way has left the snapshots half-written, so it is an error here
 // too.  The wait makes these calls synchronous; their caller synchronizes
 // right after them anyway (src/bin/jacquard.rs:1131, 1149).
-void legacy_launch(const jq_sim_args *a, uint32_t event_cap, const char *what) {
+void legacy_launch(const jq_sim_args *a0, uint32_t event_cap, const char *what) {
+  jq_sim_args a1 = *a0;
+  jq_sim_args *a = &a1;
+  legacy_depth(a);
   die_on(launch_plain(a, event_cap), what);
   const int rc = read_status(nullptr);
   if (rc == JQ_OK) return;
@@ -404,6 +629,16 @@ int jq_max_blocks(int device, size_t *max_blocks) {
 }
 
 int jq_simulate(const jq_sim_args *a) { return launch_plain(a, a ? a->event_capacity : 0); }
+
+int jq_plain_prepare(const size_t *blocks_start, const uint32_t *blocks_data, size_t num_blocks,
+                     size_t num_major_stages, uint32_t *stage_depth_base, uint8_t *stage_depth,
+                     size_t depth_capacity, size_t *num_stages, void *stream) {
+  if (!blocks_start || !blocks_data || !stage_depth_base || num_blocks == 0 ||
+      num_major_stages == 0)
+    return JQ_ERR_INVALID_ARG;
+  return plain_prepare(blocks_start, blocks_data, num_blocks, num_major_stages, stage_depth_base,
+                       stage_depth, depth_capacity, num_stages, (cudaStream_t)stream);
+}
 
 int jq_sim_status(void *stream) { return read_status(stream); }
 

@@ -21,7 +21,8 @@ class SimArgs(ctypes.Structure):
                 ("state_size", ctypes.c_size_t), ("states", vp), ("timing_constraints", vp),
                 ("events", vp), ("event_capacity", ctypes.c_uint32),
                 ("arrival_state_offset", ctypes.c_int32), ("first_cycle", ctypes.c_uint32),
-                ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp)]
+                ("barrier_timeout_cycles", ctypes.c_uint64), ("stream", vp),
+                ("stage_depth", vp), ("stage_depth_base", vp)]
 
 
 EVENT_WORDS = 8
@@ -37,6 +38,9 @@ def lib():
         L.jq_sim_status.argtypes = [vp]
         L.jq_max_blocks.restype = ctypes.c_int
         L.jq_max_blocks.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+        L.jq_plain_prepare.restype = ctypes.c_int
+        L.jq_plain_prepare.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp, vp,
+                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), vp]
         L.jq_strerror.restype = ctypes.c_char_p
         L.jq_strerror.argtypes = [ctypes.c_int]
         sz, u32p, i32 = ctypes.c_size_t, vp, ctypes.c_int32
@@ -67,6 +71,30 @@ class DeviceScript:
         self.blocks_start = torch.from_numpy(
             np.ascontiguousarray(script.blocks_start, dtype=np.uint64).view(np.int64)).to(device)
         self.blocks_data = u32_to_dev(script.blocks_data, device)
+        self._depth = None
+
+    def depth(self, stream=None):
+        """(stage depth codes, per-entry base) on the device
+        (jq_plain_prepare), computed on first use."""
+        if self._depth is None:
+            L = lib()
+            st = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+            entries = self.num_blocks * self.num_major_stages
+            base = torch.empty(entries, dtype=torch.int32, device=self.blocks_data.device)
+            n = ctypes.c_size_t()
+            rc = L.jq_plain_prepare(self.blocks_start.data_ptr(), self.blocks_data.data_ptr(),
+                                    self.num_blocks, self.num_major_stages, base.data_ptr(),
+                                    None, 0, ctypes.byref(n), st)
+            if rc:
+                raise RuntimeError("jq_plain_prepare: " + lib().jq_strerror(rc).decode())
+            depth = torch.empty(max(1, n.value), dtype=torch.uint8, device=self.blocks_data.device)
+            rc = L.jq_plain_prepare(self.blocks_start.data_ptr(), self.blocks_data.data_ptr(),
+                                    self.num_blocks, self.num_major_stages, base.data_ptr(),
+                                    depth.data_ptr(), depth.numel(), None, st)
+            if rc:
+                raise RuntimeError("jq_plain_prepare: " + lib().jq_strerror(rc).decode())
+            self._depth = (depth, base)
+        return self._depth
 
 
 def max_blocks(device=0):
@@ -79,8 +107,10 @@ def max_blocks(device=0):
 
 def simulate(ds, states, num_cycles, state_size, sram, sram_x=None, constraints=None,
              events=None, event_capacity=0, arrival_state_offset=0, first_cycle=0,
-             stream=None, barrier_timeout_cycles=0):
-    """Launch the plain interpreter (asynchronous).  All tensors on device."""
+             stream=None, barrier_timeout_cycles=0, skip_dead_levels=True):
+    """Launch the plain interpreter (asynchronous).  All tensors on device.
+    skip_dead_levels: pass the script's stage-depth tables, so tree levels
+    whose outputs nothing reads are skipped (False runs every level)."""
     a = SimArgs(ds.num_blocks, ds.num_major_stages, ds.blocks_start.data_ptr(),
                 ds.blocks_data.data_ptr(), sram.data_ptr(),
                 sram_x.data_ptr() if sram_x is not None else None, num_cycles, state_size,
@@ -88,6 +118,10 @@ def simulate(ds, states, num_cycles, state_size, sram, sram_x=None, constraints=
                 events.data_ptr() if events is not None else None, event_capacity,
                 arrival_state_offset, first_cycle, barrier_timeout_cycles,
                 stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    if skip_dead_levels:
+        depth, base = ds.depth(stream)
+        a.stage_depth = depth.data_ptr()
+        a.stage_depth_base = base.data_ptr()
     rc = lib().jq_simulate(ctypes.byref(a))
     if rc:
         raise RuntimeError("jq_simulate: " + lib().jq_strerror(rc).decode())

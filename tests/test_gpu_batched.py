@@ -32,6 +32,10 @@ def test_batched_matches_oracle_per_stream(kind, nb, split, xprop, lanes, wo_slo
     ("soc_mini", 148, (20, 40, 60), 37, 2, 0),   # one item per CTA per stage
     ("soc_mini", 148, (20, 40, 60), 37, 2, 5),   # tickets
     ("sram", 16, (8,), 4, 2, 0),
+    # lane-pair barrier groups: 3 groups of uneven size (idle CTAs included)
+    ("soc_mini", 148, (20, 40, 60), 37, 6, 0),
+    ("soc_mini", 148, (20, 40, 60), 37, 8, 0),   # 4 groups of 37, as the benchmark
+    ("soc_mini", 148, (20, 40, 60), 37, 8, 100),  # tickets: one barrier for all
 ])
 def test_batched_balanced_partitions_match_oracle(kind, nb, split, parts, lanes, grid):
     """Balanced, flat partitions (every gate at tree level 1, the batched
@@ -194,7 +198,8 @@ def test_multi_design_single_launch_matches_oracle():
 
 
 @pytest.mark.parametrize("xprop,lanes,per_item,parts", [(False, 2, 2, 0), (True, 2, 2, 0),
-                                                         (True, 1, 1, 0), (True, 2, 2, 4)])
+                                                         (True, 1, 1, 0), (True, 2, 2, 4),
+                                                         (True, 4, 2, 4)])
 def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item, parts):
     """Setup/hold checks in the batched interpreter, two launch windows of 12
     cycles: every stream's snapshots, and the multiset of (stream, event)

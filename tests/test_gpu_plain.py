@@ -18,7 +18,7 @@ REF_SO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 
 def run_gpu(s, states, cycles, sram_init=None, sram_x_init=None, constraints=None, cap=0,
-            arrival_off=0, legacy=False):
+            arrival_off=0, legacy=False, skip_dead_levels=True):
     ds = sim.DeviceScript(s)
     st = sim.u32_to_dev(states.reshape(-1))
     n_sram = max(1, s.sram_storage_size)
@@ -41,7 +41,8 @@ def run_gpu(s, states, cycles, sram_init=None, sram_x_init=None, constraints=Non
         torch.cuda.synchronize()
     else:
         sim.simulate(ds, st, cycles, states.shape[1], sram, sram_x, constraints=cons, events=ev,
-                     event_capacity=cap, arrival_state_offset=arrival_off)
+                     event_capacity=cap, arrival_state_offset=arrival_off,
+                     skip_dead_levels=skip_dead_levels)
         assert sim.status() == 0
     out = sim.dev_to_u32(st).reshape(states.shape)
     evs = sim.read_events(ev) if ev is not None else None
@@ -63,15 +64,52 @@ def sorted_events(rows):
     return sorted(map(tuple, np.asarray(rows, dtype=np.uint32).reshape(-1, 8).tolist()))
 
 
+@pytest.mark.parametrize("skip", [True, False])
 @pytest.mark.parametrize("kind,nb,split", [("tiny", 4, ()), ("tiny", 148, (5,)),
                                            ("small", 64, (8, 16, 24)), ("sram", 16, (8,))])
-def test_plain_two_state_matches_oracle(kind, nb, split):
+def test_plain_two_state_matches_oracle(kind, nb, split, skip):
     s = cases.script(kind, nb, split)
     states = cases.stimulus(kind, s, 40)
     want, wsram, _, _ = run_oracle(s, states, 40)
-    got, gsram, _, _ = run_gpu(s, states, 40)
+    got, gsram, _, _ = run_gpu(s, states, 40, skip_dead_levels=skip)
     assert np.array_equal(got, want)
     assert np.array_equal(gsram[:wsram.size], wsram)
+
+
+@pytest.mark.parametrize("kind,nb,split,parts,xprop,timed", [
+    ("soc_mini", 148, (20, 40, 60), 37, True, False),
+    ("sram", 16, (8,), 4, True, False),
+    ("sram", 16, (8,), 4, False, True),
+    ("small", 148, (8, 16, 24), 37, False, False),
+])
+def test_plain_balanced_scripts_skip_dead_levels(kind, nb, split, parts, xprop, timed):
+    """Balanced scripts evaluate only the first AND level of every stage, so
+    their stage-depth codes are all 0 and the plain interpreter skips the
+    deeper levels and their barriers: snapshots (arrivals included) and the
+    violation multiset still equal the oracle's."""
+    s = cases.script(kind, nb, split, xprop=xprop, timing_seed=9 if timed else 0,
+                     target_parts=parts)
+    ds = sim.DeviceScript(s)
+    depth, _ = ds.depth()
+    assert int(depth.max()) == 0
+    if timed:
+        s.enable_timing_arrivals()
+    try:
+        states = cases.stimulus(kind, s, 24, x_init=xprop)
+        cons = cases.constraint_buffer(kind, s, clock_ps=120, setup=30, hold=150) if timed else None
+        off = s.arrival_state_offset if timed else 0
+        want, wsram, _, (wev, wcnt) = run_oracle(s, states, 24, constraints=cons,
+                                                 cap=1 << 16 if timed else 0, arrival_off=off)
+        got, gsram, _, evs = run_gpu(s, states, 24, constraints=cons, cap=1 << 16 if timed else 0,
+                                     arrival_off=off)
+    finally:
+        s.timing_arrivals_enabled = False
+        s.arrival_state_offset = 0
+    assert np.array_equal(got, want)
+    assert np.array_equal(gsram[:wsram.size], wsram)
+    if timed:
+        assert evs[1] == wcnt and wcnt > 0
+        assert sorted_events(evs[0]) == sorted_events(wev.view(np.uint32))
 
 
 @pytest.mark.parametrize("kind,nb,split", [("tiny", 8, (5,)), ("sram", 16, (8,))])
