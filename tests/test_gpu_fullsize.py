@@ -131,14 +131,15 @@ def test_batched_256_streams_match_plain_and_oracle(soc):
 def test_benchmark_script_and_stimulus_256_streams_64_cycles():
     """The exact configuration bench.py times: its design, its script
     (148 blocks, balanced partitions, at most 37 per major stage, flat stages
-    in the compact form), its stimulus (16 reset cycles, then p_toggle 0.25,
+    in the compact form, the cut bench.py picks), its stimulus (16 reset cycles, then p_toggle 0.25,
     stream k seeded 1000 + k) and one of its 64-cycle windows with the
     output waveform, 256 streams: every snapshot of every stream against the
     plain interpreter, two streams against the oracle."""
     import bench
     d = bench.build_design()
-    s = bench.build_script(d, 148, target_parts=37)
-    assert s.num_partitions == 740
+    model = bench.learned_model() if bench.learned_wins() else None  # as bench.py decides
+    s = bench.build_script(d, 148, target_parts=37, cost_model=model)
+    assert s.num_partitions <= 740
     assert int(s.features[:, 14].max()) <= 1  # flat stages: the compact form
     cycles = 64
     packed = []

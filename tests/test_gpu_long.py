@@ -122,7 +122,8 @@ class LaneStimulus:
 def test_soc_100k_cycles_256_streams_windowed():
     import bench
     d = bench.build_design()
-    s = bench.build_script(d, 148, target_parts=37)
+    model = bench.learned_model() if bench.learned_wins() else None  # as bench.py decides
+    s = bench.build_script(d, 148, target_parts=37, cost_model=model)
     lanes, W, total = 8, 2000, 100_000 + bench.RESET_CYCLES
     total -= total % W  # whole windows: 100,000 cycles
     streams = 32 * lanes
