@@ -725,33 +725,60 @@ def multi_design_sizes(n=12, lo=50_000, hi=4_000_000, seed=4):
 def run_mine_multi(args, rank, world):
     """Twelve designs of log-uniform size in [50k, 4M] AND nodes in one
     persistent launch (scripts relocated into one), replayed from a CUDA
-    graph; 8 lane words (256 streams) per design."""
+    graph; 8 lane words (256 streams) per design, each stream with its own
+    random stimulus (p_toggle 0.25), every design's primary outputs recorded
+    each cycle.  e2e: the stimulus copied in and the waveform copied out
+    around every replay."""
     import torch
-    from jacquard_b200 import batched
+    from jacquard_b200 import batched, state
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     sizes = multi_design_sizes()
-    scripts, ands = [], 0
+    scripts, designs, ands = [], [], 0
     for k, n_and in enumerate(sizes.tolist()):
         clusters = max(1, int(round(n_and / 4096)))
         d = build_design(seed=40 + 100 * rank + k, clusters=clusters,
                          n_dff=max(64, 200_000 * clusters // 512))
         ands += int(d.num_and)
         scripts.append(build_script(d, 148))
+        designs.append(d)
     comb = batched.CombinedScript(scripts)
     lanes = args.lanes
-    B = batched.BatchedSim(comb, lanes, device=dev)
-    B.load_state(np.zeros((lanes, B.sig), np.uint32))
-    B.reset_sram(x=True)
     W = args.window
+    po_sig = np.concatenate([[comb.signal(i, int(p)) for p in state.po_positions(s, d)]
+                             for i, (s, d) in enumerate(zip(scripts, designs))]).astype(np.int64)
+    B = batched.BatchedSim(comb, lanes, device=dev, po_signals=po_sig)
+    # stimulus: each design's input lane words, concatenated per lane
+    rng = np.random.default_rng(4000 + rank)
+    rows = np.zeros((W + 1, lanes, B.in_sigs), np.uint32)
+    col = 0
+    for s, d in zip(scripts, designs):
+        pos = state.input_positions(s)
+        lay = np.asarray(s.input_layout)
+        cur = rng.integers(0, 2**32, size=(lanes, pos.size), dtype=np.uint32)
+        for c in range(W + 1):
+            if c:
+                cur ^= (rng.integers(0, 2**32, size=cur.shape, dtype=np.uint32)
+                        & rng.integers(0, 2**32, size=cur.shape, dtype=np.uint32))
+            v = cur.copy()
+            v[:, lay == d.clock_flag_pin] = 0xFFFFFFFF
+            rows[c, :, col + pos] = v
+        col += batched.input_words(s) * 32
+    B.load_state(np.zeros((lanes, B.sig), np.uint32))  # known zero state; inputs from cycle 1
+    B.reset_sram(x=True)
+    stim_pin = torch.from_numpy(np.ascontiguousarray(rows).reshape(-1).view(np.int32)).pin_memory()
+    stim_dev = torch.empty(stim_pin.numel(), dtype=torch.int32, device=dev)
+    stim_dev.copy_(stim_pin)
+    wave = torch.empty(W * len(po_sig) * lanes, dtype=torch.int32, device=dev)
+    wave_pin = torch.empty(wave.numel(), dtype=torch.int32).pin_memory()
     stream = torch.cuda.Stream(dev)
     with torch.cuda.stream(stream):
-        B.run(None, W, stream=stream)
+        B.run(stim_dev, W, wave=wave, stream=stream)
         stream.synchronize()
         assert B.status(stream) == 0
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=stream):
-            B.run(None, W, stream=stream)
+            B.run(stim_dev, W, wave=wave, stream=stream)
     for _ in range(args.warmup):
         g.replay()
     torch.cuda.synchronize()
@@ -768,13 +795,27 @@ def run_mine_multi(args, rank, world):
         timed_region_edge(world)
     dev_ms = t0.elapsed_time(t1)
     assert B.status(stream) == 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    timed_region_edge(world)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            stim_dev.copy_(stim_pin, non_blocking=True)
+            g.replay()
+            wave_pin.copy_(wave, non_blocking=True)
+    e1.record(stream)
+    timed_region_edge(world)
+    e2e_ms = e0.elapsed_time(e1)
+    assert B.status(stream) == 0
+    del g
     streams = 32 * lanes * len(scripts)
     per = [algorithmic_bytes_per_cycle(s, streams=32 * lanes, bit_sliced=True) for s in scripts]
     bytes_per_cycle = sum(p[0] + p[1] for p in per)
-    return dict(dev_ms=dev_ms, e2e_ms=None, cycles_per_step=W, streams=streams,
+    return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams,
                 clocks=ck.summary(), bytes_per_cycle=bytes_per_cycle,
                 script_bytes=sum(p[0] for p in per), kernel_ms=dev_ms / args.steps,
-                h2d=0, d2h=0, launches_per_step=2,
+                h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4, launches_per_step=2,
                 design=dict(designs=len(scripts), ands=ands, sizes=sizes.tolist(),
                             partitions=int(sum(s.num_partitions for s in scripts)),
                             script_mb_per_cycle=comb.script_words_per_cycle() * 4 / 1e6,
