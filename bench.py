@@ -762,7 +762,7 @@ def run_mine_multi(args, rank, world):
                         & rng.integers(0, 2**32, size=cur.shape, dtype=np.uint32))
             v = cur.copy()
             v[:, lay == d.clock_flag_pin] = 0xFFFFFFFF
-            rows[c, :, col + pos] = v
+            rows[c][:, col + pos] = v
         col += batched.input_words(s) * 32
     B.load_state(np.zeros((lanes, B.sig), np.uint32))  # known zero state; inputs from cycle 1
     B.reset_sram(x=True)

@@ -1508,6 +1508,11 @@ struct PrepShared {
   uint16_t slot_cur[8192];
   uint16_t pos_of[4096];    // region slot -> position
   uint8_t live[8192];
+  // bank-aware slot order of a compact stage (see below)
+  uint8_t bucket_of[4096];  // entry -> 9 * (a bank group) + (b bank group), 8 = no load
+  uint16_t sorted[4096];    // entries by bucket
+  uint16_t order[4096];     // new slot -> entry
+  uint16_t bcnt[81], bptr[81];
 };
 
 // Exclusive prefix sum of v over the CTA; *total receives the sum.  Every
@@ -1831,6 +1836,70 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
           }
         }
         __syncthreads();
+        // Bank-aware order of the slots no hook reads ([32 nh, n)).  A gather
+        // of the kernel's compact stage reads 16 bytes per lane, and the 8
+        // lanes of a quarter warp are served in one wavefront when their
+        // addresses fall in distinct 16-byte bank groups (word mod 8).  Each
+        // group of 8 slots (a quarter warp: the region starts 32-aligned
+        // after the hooked blocks) takes entries whose a sources, and whose b
+        // sources, lie in distinct bank groups where the remaining entries
+        // allow it (greedy, fullest bucket first).
+        {
+          const uint32_t h0 = 32 * nh, m = n - h0;
+          for (uint32_t i = t; i < m; i += BT) {
+            const uint32_t P = ps.pos_of[h0 + i];
+            const uint32_t ob = (C[4096 + 4 * (P >> 5) + 2] >> (P & 31)) & 1u;
+            const uint32_t sa = perm_src(C, P - 4096) & 8191u, sb = perm_src(C, P) & 8191u;
+            const uint32_t ra = (ci > 0 && sa == 0) ? REF_ZERO : ps.slot_prev[sa];
+            const uint32_t rb = (ob || (ci > 0 && sb == 0)) ? REF_ZERO : ps.slot_prev[sb];
+            const uint32_t ba = ra >= REF_ONE ? 8u : (ra & 7u), bb = rb >= REF_ONE ? 8u : (rb & 7u);
+            ps.bucket_of[i] = (uint8_t)(9 * ba + bb);
+          }
+          if (t < 81) ps.bcnt[t] = 0;
+          __syncthreads();
+          if (t == 0 && m > 8) {
+            for (uint32_t i = 0; i < m; ++i) ++ps.bcnt[ps.bucket_of[i]];
+            uint32_t acc = 0;
+            for (int b = 0; b < 81; ++b) {
+              ps.bptr[b] = (uint16_t)acc;
+              acc += ps.bcnt[b];
+            }
+            for (uint32_t i = 0; i < m; ++i) ps.sorted[ps.bptr[ps.bucket_of[i]]++] = (uint16_t)i;
+            for (int b = 0; b < 81; ++b) ps.bptr[b] = (uint16_t)(ps.bptr[b] - ps.bcnt[b]);
+            for (uint32_t g = 0; g < m; g += 8) {
+              uint32_t used_a = 0, used_b = 0;
+              for (uint32_t k = 0; k < 8 && g + k < m; ++k) {
+                int best = -1, any = -1;
+                uint32_t best_c = 0, any_c = 0;
+                for (int b = 0; b < 81; ++b) {
+                  const uint32_t c = ps.bcnt[b];
+                  if (!c) continue;
+                  if (c > any_c) { any = b; any_c = c; }
+                  const uint32_t ba = (uint32_t)b / 9, bb = (uint32_t)b % 9;
+                  const bool free_a = ba == 8 || !((used_a >> ba) & 1u);
+                  const bool free_b = bb == 8 || !((used_b >> bb) & 1u);
+                  if (free_a && free_b && c > best_c) { best = b; best_c = c; }
+                }
+                if (best < 0) best = any;
+                ps.order[g + k] = ps.sorted[ps.bptr[best] + --ps.bcnt[best]];
+                const uint32_t ba = (uint32_t)best / 9, bb = (uint32_t)best % 9;
+                if (ba < 8) used_a |= 1u << ba;
+                if (bb < 8) used_b |= 1u << bb;
+              }
+            }
+          } else if (t == 0) {
+            for (uint32_t i = 0; i < m; ++i) ps.order[i] = (uint16_t)i;
+          }
+          __syncthreads();
+          for (uint32_t i = t; i < m; i += BT) ps.sorted[i] = ps.pos_of[h0 + ps.order[i]];
+          __syncthreads();
+          for (uint32_t i = t; i < m; i += BT) {
+            const uint32_t P = ps.sorted[i];
+            ps.pos_of[h0 + i] = (uint16_t)P;
+            ps.slot_cur[P] = (uint16_t)(base + h0 + i);
+          }
+          __syncthreads();
+        }
         for (uint32_t i = t; i < n; i += BT) {
           const uint32_t P = ps.pos_of[i];
           const uint32_t *F = C + 4096 + 4 * (P >> 5);
