@@ -350,3 +350,47 @@ def test_launches_on_two_streams_overlap_safely():
         assert sim.status(stream) == 0
         assert np.array_equal(sim.dev_to_u32(st).reshape(shape), want)
         assert np.array_equal(sim.dev_to_u32(sram)[:wsram.size], wsram)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference kernel not built")
+def test_drop_in_symbol_outruns_reference_kernel():
+    """The benchmark's 2M-gate SoC, one stream, the cone-6000 script for 296
+    blocks (the reference's 2 CTAs per SM): the reference's kernel through
+    its own symbol and this library's same-named symbol, same buffers, 16
+    cycles, best of three.  Both end in the same snapshots; this library's
+    is faster.  Prints both rates."""
+    import time
+    import bench
+    d = bench.build_design()
+    s = bench.build_script(d, 296)
+    W = 16
+    host = bench.stimulus_window(s, d, 0, W, seed=100)
+    eff = host.shape[1]
+    L = ctypes.CDLL(REF_SO)
+    sz, vp = ctypes.c_size_t, ctypes.c_void_p
+    L.simulate_v1_noninteractive_simple_scan_cuda.argtypes = [sz, sz, vp, vp, vp, vp, sz, sz, vp,
+                                                              ctypes.c_int32]
+    ds = sim.DeviceScript(s)
+    n_sram = max(1, s.sram_storage_size)
+    rates, finals = {}, {}
+    for who, fn in (("reference", L.simulate_v1_noninteractive_simple_scan_cuda),
+                    ("this", sim.lib().simulate_v1_noninteractive_simple_scan_cuda)):
+        best = None
+        for _ in range(4):  # the first run warms up
+            st = sim.u32_to_dev(host.reshape(-1))
+            sram = torch.zeros(n_sram, dtype=torch.int32, device="cuda")
+            sram_x = torch.full((n_sram,), -1, dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn(s.num_blocks, s.num_major_stages, ds.blocks_start.data_ptr(), ds.blocks_data.data_ptr(),
+               sram.data_ptr(), sram_x.data_ptr(), W, eff, st.data_ptr(), 0)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        rates[who] = W / best
+        finals[who] = (sim.dev_to_u32(st), sim.dev_to_u32(sram), sim.dev_to_u32(sram_x))
+    print(f"cycles/s: reference kernel {rates['reference']:.0f}, this library {rates['this']:.0f}, "
+          f"ratio {rates['this'] / rates['reference']:.3f}")
+    for a, b in zip(finals["reference"], finals["this"]):
+        assert np.array_equal(a, b)
+    assert rates["this"] > rates["reference"], rates
