@@ -56,28 +56,45 @@ def lib():
     return L
 
 
+# (shift, mask) rounds of a 32x32 bit-matrix transpose by block swaps: the
+# off-diagonal 16x16 blocks, then within each the 8x8 ones, down to single
+# bits.
+_T32_ROUNDS = ((16, 0x0000FFFF), (8, 0x00FF00FF), (4, 0x0F0F0F0F), (2, 0x33333333),
+               (1, 0x55555555))
+
+
+def _transpose32(x):
+    """(..., 32) u32 -> (..., 32) u32 with bit i of out[..., b] = bit b of
+    x[..., i] (a copy)."""
+    x = np.array(x, dtype=np.uint32, copy=True)
+    for j, m in _T32_ROUNDS:
+        xr = x.reshape(x.shape[:-1] + (32 // (2 * j), 2, j))
+        a, b = xr[..., 0, :], xr[..., 1, :]
+        t = ((a >> np.uint32(j)) ^ b) & np.uint32(m)
+        b ^= t
+        a ^= t << np.uint32(j)
+    return x
+
+
 def to_batched(per_stream):
     """(streams, ..., words) u32 per-stream layout -> (..., lanes, words*32)
     lane-major lane words: word [l, signal] holds `signal` of streams
     32l..32l+31 (bit i = stream 32l+i).  streams must be a multiple of 32."""
     a = np.asarray(per_stream, dtype=np.uint32)
-    S = a.shape[0]
+    S, W = a.shape[0], a.shape[-1]
     assert S % 32 == 0
-    bits = ((a[..., None] >> np.arange(32, dtype=np.uint32)) & 1).astype(np.uint8)
-    bits = bits.reshape(a.shape[:-1] + (a.shape[-1] * 32,))       # (S, ..., sig)
-    bits = np.moveaxis(bits, 0, -1)                                # (..., sig, S)
-    packed = np.packbits(bits, axis=-1, bitorder="little")        # (..., sig, S/8)
-    words = np.ascontiguousarray(packed).view(np.uint32)          # (..., sig, lanes)
-    return np.ascontiguousarray(np.swapaxes(words, -1, -2))      # (..., lanes, sig)
+    x = np.moveaxis(a.reshape((S // 32, 32) + a.shape[1:]), (0, 1), (-3, -1))  # (..., lanes, W, 32)
+    y = _transpose32(x)
+    return np.ascontiguousarray(y.reshape(y.shape[:-2] + (W * 32,)))
 
 
 def from_batched(batched, words):
     """Inverse of to_batched: (..., lanes, sig) -> (streams, ..., words)."""
-    b = np.ascontiguousarray(np.swapaxes(np.asarray(batched, dtype=np.uint32), -1, -2))
-    bits = np.unpackbits(b.view(np.uint8), axis=-1, bitorder="little")  # (..., sig, S)
-    bits = np.moveaxis(bits, -1, 0).astype(np.uint32)              # (S, ..., sig)
-    bits = bits.reshape(bits.shape[:-1] + (words, 32))
-    return (bits << np.arange(32, dtype=np.uint32)).sum(axis=-1, dtype=np.uint64).astype(np.uint32)
+    b = np.asarray(batched, dtype=np.uint32)
+    lanes = b.shape[-2]
+    y = _transpose32(b.reshape(b.shape[:-1] + (words, 32)))         # (..., lanes, W, 32)
+    y = np.moveaxis(y, (-3, -1), (0, 1))                            # (lanes, 32, ..., W)
+    return np.ascontiguousarray(y.reshape((lanes * 32,) + y.shape[2:]))
 
 
 def input_words(script):

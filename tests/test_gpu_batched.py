@@ -1,4 +1,6 @@
 """Batched (bit-lane) interpreter vs the CPU oracle run stream by stream."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -8,6 +10,8 @@ import oracle_lib
 from jacquard_b200 import batched, state
 
 pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
 
 
 @pytest.mark.parametrize("kind,nb,split,xprop,lanes,wo_slots,per_item,grid", [
@@ -62,7 +66,7 @@ class BatchedCase:
             st = self.want[k].reshape(-1).copy()
             sram = np.zeros(max(1, s.sram_storage_size), np.uint32)
             sram_x = np.full_like(sram, 0xFFFFFFFF)
-            oracle_lib.simulate(s, st, cycles, self.eff, sram=sram, sram_x=sram_x)
+            oracle_lib.simulate(s, st, cycles, self.eff, sram=sram, sram_x=sram_x, threads=THREADS)
             self.want[k] = st.reshape(cycles + 1, self.eff)
             self.wsram.append(sram)
         self.B = batched.BatchedSim(s, lanes, record=True, wo_slots=wo_slots,
@@ -190,7 +194,7 @@ def test_multi_design_single_launch_matches_oracle():
             want = snaps[d][k].reshape(-1).copy()
             osram = np.zeros(n_sram, np.uint32)
             osram_x = np.full(n_sram, 0xFFFFFFFF, np.uint32)
-            oracle_lib.simulate(s, want, cycles, eff, sram=osram, sram_x=osram_x)
+            oracle_lib.simulate(s, want, cycles, eff, sram=osram, sram_x=osram_x, threads=THREADS)
             assert np.array_equal(got[k].reshape(-1), want), f"design {d} stream {k}"
             if s.sram_storage_size:
                 b = C.sram_base[d]

@@ -33,7 +33,7 @@ def test_small_design_4096_cycles_plain_and_batched():
     s = cases.script("small", 64, (8, 16, 24))
     states = cases.stimulus("small", s, cycles, seed=1)
     want = states.reshape(-1).copy()
-    oracle_lib.simulate(s, want, cycles, states.shape[1])
+    oracle_lib.simulate(s, want, cycles, states.shape[1], threads=THREADS)
     ds = sim.DeviceScript(s)
     st = sim.u32_to_dev(states.reshape(-1))
     sram = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -66,7 +66,7 @@ def test_small_design_4096_cycles_plain_and_batched():
         assert np.array_equal(got[k], plain), f"stream {k}: batched != plain"
         if k % 21 == 0:  # streams 0, 21, 42, 63
             o = snaps[k].reshape(-1).copy()
-            oracle_lib.simulate(sb, o, cycles, eff)
+            oracle_lib.simulate(sb, o, cycles, eff, threads=THREADS)
             assert np.array_equal(plain.reshape(-1), o), f"stream {k}: plain != oracle"
 
 
