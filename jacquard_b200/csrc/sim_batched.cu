@@ -692,8 +692,7 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           WO[(num_ios - num_srams - num_dup) * 32 + q] = St[num_srams * 4 * 32 + q];
         __syncthreads();
       } else {
-        // ---------------- clock-enable permutation and commit (4 words per
-        // thread in flight)
+        // ---------------- clock-enable permutation and commit
         JQ_FAIL_IF(!ok)
         // the item's last commit: take the next work ticket now, so its
         // latency overlaps the commit
@@ -703,48 +702,35 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         }
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
-        for (uint32_t q0 = t; q0 < nq; q0 += 4 * BT) {
-          uint32_t cp[4], cpx[4], wv[4], wx[4], old[4], oldx[4];
-          size_t sg[4];
-#pragma unroll
-          for (int uu = 0; uu < 4; ++uu) {
-            const uint32_t q = q0 + uu * BT;
-            if (q < nq) {
-              const uint2 src = WO[perm_lin(C, q)];
-              const uint4 fl = F4[q >> 5];
-              const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q),
-                             dinv = bitmask(fl.z, q);
-              const uint2 me = WO[q];
-              cp[uu] = (src.x & ~set0) ^ inv;
-              cpx[uu] = is_x ? (src.y & ~set0) : 0u;
-              if (P.constraints)  // a warp holds the 32 signals of one word
-                check_word(P, io_off + (q >> 5), __reduce_or_sync(0xffffffffu, cp[uu]), lane,
-                           0u, 0u, P.first_cycle + cyc, cyc == 0);
-              wv[uu] = me.x ^ dinv;
-              wx[uu] = me.y;
-              sg[uu] = lane_base + (((size_t)io_off * 32 + q) << sig_shift);
-              if (is_x) {  // quad layout: (v, x) adjacent
-                const uint2 o = __ldcg(reinterpret_cast<const uint2 *>(in + sg[uu]));
-                old[uu] = o.x;
-                oldx[uu] = o.y;
-              } else {
-                old[uu] = ldcg(in + sg[uu]);
-                oldx[uu] = 0u;
-              }
+        // the old word is loaded only by warps where some stream of their
+        // state word keeps its value (clock enable clear): none, when every
+        // enable is set
+        for (uint32_t q = t; q < nq; q += BT) {  // warp-uniform bound
+          const uint2 src = WO[perm_lin(C, q)];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q), dinv = bitmask(fl.z, q);
+          const uint2 me = WO[q];
+          const uint32_t cp = (src.x & ~set0) ^ inv, cpx = is_x ? (src.y & ~set0) : 0u;
+          if (P.constraints)  // a warp holds the 32 signals of one word
+            check_word(P, io_off + (q >> 5), __reduce_or_sync(0xffffffffu, cp), lane, 0u, 0u,
+                       P.first_cycle + cyc, cyc == 0);
+          const size_t sg = lane_base + (((size_t)io_off * 32 + q) << sig_shift);
+          uint32_t old = 0, oldx = 0;
+          if (__any_sync(0xffffffffu, cp != 0xffffffffu)) {
+            if (is_x) {  // quad layout: (v, x) adjacent
+              const uint2 o = __ldcg(reinterpret_cast<const uint2 *>(in + sg));
+              old = o.x;
+              oldx = o.y;
+            } else {
+              old = ldcg(in + sg);
             }
           }
-#pragma unroll
-          for (int uu = 0; uu < 4; ++uu) {
-            const uint32_t q = q0 + uu * BT;
-            if (q < nq) {
-              const uint32_t nv = (old[uu] & ~cp[uu]) | (wv[uu] & cp[uu]);
-              if (is_x)
-                *reinterpret_cast<uint2 *>(out + sg[uu]) = make_uint2(
-                    nv, (oldx[uu] & ~cp[uu] & ~cpx[uu]) | (wx[uu] & cp[uu] & ~cpx[uu]) | cpx[uu]);
-              else
-                out[sg[uu]] = nv;
-            }
-          }
+          const uint32_t nv = (old & ~cp) | ((me.x ^ dinv) & cp);
+          if (is_x)
+            *reinterpret_cast<uint2 *>(out + sg) =
+                make_uint2(nv, (oldx & ~cp & ~cpx) | (me.y & cp & ~cpx) | cpx);
+          else
+            out[sg] = nv;
         }
       }
     }
@@ -1125,58 +1111,47 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         }
         const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
-        // the old words of up to 4 q per thread are loaded before any store,
-        // so their latencies overlap
-        for (uint32_t q0 = t; q0 < nq; q0 += 2 * BT) {
-          uint32_t o[2][4];  // old v0, v1, x0, x1
-#pragma unroll
-          for (int uu = 0; uu < 2; ++uu) {
-            const uint32_t q = q0 + uu * BT;
-            if (q < nq) {
-              const size_t sg = (size_t)io_off * 32 + q;
-              if (is_x) {  // quad layout
-                const uint4 w = __ldcg(reinterpret_cast<const uint4 *>(in + pair_base + (sg << 2)));
-                o[uu][0] = w.x;
-                o[uu][1] = w.z;
-                o[uu][2] = w.y;
-                o[uu][3] = w.w;
-              } else {
-                const size_t w = pair_base + (sg << (P.xhalf ? 2 : 1));
-                o[uu][0] = ldcg(in + w);
-                o[uu][1] = ldcg(in + w + (P.xhalf ? 2 : 1));
-                o[uu][2] = o[uu][3] = 0u;
-              }
+        // The new words come from shared memory; the old words (kept by
+        // streams whose clock enable is clear) are loaded only by warps where
+        // some stream of their state word keeps its value -- none, when
+        // every enable is set.
+        for (uint32_t q = t; q < nq; q += BT) {  // warp-uniform bound
+          const uint4 src = WO[perm_lin(C, q)];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q), dinv = bitmask(fl.z, q);
+          const uint4 me = WO[q];
+          const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
+          if (P.constraints)  // a warp holds the 32 signals of one word
+            check_word(P, io_off + (q >> 5), __reduce_or_sync(0xffffffffu, cp0), 2 * lp,
+                       __reduce_or_sync(0xffffffffu, cp1), 2 * lp + 1, P.first_cycle + cyc,
+                       cyc == 0);
+          const size_t sg = (size_t)io_off * 32 + q;
+          uint32_t o0 = 0, o1 = 0, ox0 = 0, ox1 = 0;  // old v0, v1, x0, x1
+          if (__any_sync(0xffffffffu, (cp0 & cp1) != 0xffffffffu)) {
+            if (is_x) {  // quad layout
+              const uint4 w = __ldcg(reinterpret_cast<const uint4 *>(in + pair_base + (sg << 2)));
+              o0 = w.x;
+              ox0 = w.y;
+              o1 = w.z;
+              ox1 = w.w;
+            } else {
+              const size_t w = pair_base + (sg << (P.xhalf ? 2 : 1));
+              o0 = ldcg(in + w);
+              o1 = ldcg(in + w + (P.xhalf ? 2 : 1));
             }
           }
-#pragma unroll
-          for (int uu = 0; uu < 2; ++uu) {
-            const uint32_t q = q0 + uu * BT;
-            if (q < nq) {
-              const uint4 src = WO[perm_lin(C, q)];
-              const uint4 fl = F4[q >> 5];
-              const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q),
-                             dinv = bitmask(fl.z, q);
-              const uint4 me = WO[q];
-              const size_t sg = (size_t)io_off * 32 + q;
-              const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
-              if (P.constraints)  // a warp holds the 32 signals of one word
-                check_word(P, io_off + (q >> 5), __reduce_or_sync(0xffffffffu, cp0), 2 * lp,
-                           __reduce_or_sync(0xffffffffu, cp1), 2 * lp + 1, P.first_cycle + cyc,
-                           cyc == 0);
-              const uint32_t n0 = (o[uu][0] & ~cp0) | ((me.x ^ dinv) & cp0);
-              const uint32_t n1 = (o[uu][1] & ~cp1) | ((me.z ^ dinv) & cp1);
-              if (is_x) {
-                const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
-                *reinterpret_cast<uint4 *>(out + pair_base + (sg << 2)) =
-                    make_uint4(n0, (o[uu][2] & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0, n1,
-                               (o[uu][3] & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1);
-              } else if (P.xhalf) {  // values only; the X words keep theirs
-                out[pair_base + (sg << 2)] = n0;
-                out[pair_base + (sg << 2) + 2] = n1;
-              } else {
-                *reinterpret_cast<uint2 *>(out + pair_base + (sg << 1)) = make_uint2(n0, n1);
-              }
-            }
+          const uint32_t n0 = (o0 & ~cp0) | ((me.x ^ dinv) & cp0);
+          const uint32_t n1 = (o1 & ~cp1) | ((me.z ^ dinv) & cp1);
+          if (is_x) {
+            const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
+            *reinterpret_cast<uint4 *>(out + pair_base + (sg << 2)) =
+                make_uint4(n0, (ox0 & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0, n1,
+                           (ox1 & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1);
+          } else if (P.xhalf) {  // values only; the X words keep theirs
+            out[pair_base + (sg << 2)] = n0;
+            out[pair_base + (sg << 2) + 2] = n1;
+          } else {
+            *reinterpret_cast<uint2 *>(out + pair_base + (sg << 1)) = make_uint2(n0, n1);
           }
         }
       }
