@@ -439,14 +439,14 @@ def run_mine_batched(args, rank, world):
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
     use_learned = args.learned == "on" or (args.learned == "auto" and learned_wins())
     model = learned_model() if use_learned else None
-    s = build_script(d, args.blocks, cost_model=model,
-                     target_parts=args.blocks // max(1, args.lanes // 2))
+    per_stage = args.blocks // max(1, args.lanes // args.per_item)  # one round of items
+    s = build_script(d, args.blocks, cost_model=model, target_parts=per_stage)
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
     assert W % 2 == 0, "even windows keep the final state in buffer A"
     po_sig = state.po_positions(s, d)
-    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
+    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig, lanes_per_item=args.per_item)
     # snapshot 0: inputs of cycle 0, every DFF/SRAM word X
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
     snap0 = np.zeros((lanes, B.sig), np.uint32)
@@ -508,8 +508,9 @@ def run_mine_batched(args, rank, world):
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
                             script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
+                            lanes_per_item=args.per_item,
                             partitioner="balanced: at most %d per major stage%s"
-                            % (args.blocks // max(1, args.lanes // 2),
+                            % (per_stage,
                                ", cut chosen by the learned cost model" if model is not None
                                else ", heuristic cut")),
                 script=s, d=d)
@@ -881,6 +882,8 @@ def main():
                     help="timed: event records per window")
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
+    ap.add_argument("--per-item", type=int, default=2, choices=[2, 8],
+                    help="batched: lane words per work item (2: lane pairs, 8: octets)")
     ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
     ap.add_argument("--cpu-cycles", type=int, default=160,
                     help="CPU baseline sample: cycles of one stream (about 10 s single-threaded)")

@@ -152,11 +152,16 @@ int jq_max_blocks(int device, size_t *max_blocks);
 /* Bit-lane batched interpreter: 32*lanes independent stimulus streams run the
  * same script in one persistent launch.  A lane word holds one signal (a bit
  * position of the reference layout, word*32+bit, X plane at metadata word
- * 9 * 32) for streams 32l..32l+31.  The state buffers interleave lane pairs
+ * 9 * 32) for streams 32l..32l+31.  The state buffers interleave lane groups
  * (jq_batched_state_words words; lanes rounded up to even):
- *   x_interleaved = 1 (V = signals_per_snapshot / 2 value signals, signal
- *     V + s the X of s): word ((l >> 1) * V + s mod V) * 4 + 2 * (l & 1) +
- *     (s >= V), i.e. (value, X) of the even lane, then of the odd lane;
+ *   x_interleaved = 1, lane-pair quads (V = signals_per_snapshot / 2 value
+ *     signals, signal V + s the X of s): word ((l >> 1) * V + s mod V) * 4 +
+ *     2 * (l & 1) + (s >= V), i.e. (value, X) of the even lane, then of the
+ *     odd lane;
+ *   x_interleaved = 2, lane octets (lanes a multiple of 8): word
+ *     ((l >> 3) * V + s mod V) * 16 + 2 * (l & 7) + (s >= V), i.e. the 64
+ *     bytes (value, X) of 8 lane words for one signal are adjacent; it runs
+ *     octet work items (lanes_per_item 8) only;
  *   x_interleaved = 0: word ((l >> 1) * signals + s) * 2 + (l & 1).
  * jq_batched_pack_state / jq_batched_unpack_state convert from / to the
  * lane-major form [l][signal] that `stimulus`, `wave` and `record` use.
@@ -211,13 +216,20 @@ typedef struct {
   uint64_t barrier_timeout_cycles;
   void *stream;
   uint32_t lanes_per_item;     /* lane words one work item runs: 0 = automatic
-                                  (2 when lanes is even and the shared memory
-                                  of a lane pair fits the writeouts, else 1),
-                                  1, or 2 (JQ_ERR_INVALID_ARG when it does not
-                                  fit or lanes is odd) */
-  int32_t x_interleaved;       /* state layout (below): 1 when signals
-                                  [S/2, S) are the X planes of [0, S/2)
-                                  (S = signals_per_snapshot; required when any
+                                  (8 in the octet layout; otherwise 2 when
+                                  lanes is even and the shared memory of a
+                                  lane pair fits the writeouts, else 1), 1, 2,
+                                  or 8 (JQ_ERR_INVALID_ARG when it does not
+                                  fit, lanes does not divide, or the layout
+                                  differs).  Octet items need every partition
+                                  in the compact form the prepare step writes
+                                  and within jq_batched_oct_capacity slots
+                                  (jq_batched_slot_need); a partition that is
+                                  not gives JQ_ERR_INVALID_ARG in the status */
+  int32_t x_interleaved;       /* state layout (above): 1 (lane-pair quads) or
+                                  2 (lane octets) when signals [S/2, S) are
+                                  the X planes of [0, S/2) (S =
+                                  signals_per_snapshot; required when any
                                   partition is X-capable, and then every such
                                   partition's X offset, metadata word 9, is
                                   S/64 words), 0 for scripts without X */
@@ -271,6 +283,14 @@ int jq_batched_unpack_state(const uint32_t *state, uint32_t lanes, size_t signal
 int jq_batched_status(void *stream);
 int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks);
 int jq_batched_smem_bytes(uint32_t wo_slots);
+/* Octet work items (no counterpart in the reference): the 64-byte tree slots
+ * one item holds in shared memory on the current device, and, into the
+ * device word *need (asynchronous on `stream`), the most slots any partition
+ * of a prepared script needs (0xffffffff when some partition cannot run as an
+ * octet item).  Octet items run a script when need <= capacity. */
+int jq_batched_oct_capacity(uint32_t *slots);
+int jq_batched_slot_need(const size_t *blocks_start, const uint32_t *prepared, size_t num_blocks,
+                         size_t num_major_stages, uint32_t *need, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* Partition cost model (no counterpart in the reference): an MLP

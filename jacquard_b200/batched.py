@@ -52,6 +52,10 @@ def lib():
         for fn in (L.jq_batched_pack_state, L.jq_batched_unpack_state):
             fn.restype = ctypes.c_int
             fn.argtypes = [vp, ctypes.c_uint32, ctypes.c_size_t, ctypes.c_int32, vp, vp]
+        L.jq_batched_oct_capacity.restype = ctypes.c_int
+        L.jq_batched_oct_capacity.argtypes = [ctypes.POINTER(ctypes.c_uint32)]
+        L.jq_batched_slot_need.restype = ctypes.c_int
+        L.jq_batched_slot_need.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp, vp]
         L._jq_batched_typed = True
     return L
 
@@ -74,6 +78,15 @@ def _transpose32(x):
         b ^= t
         a ^= t << np.uint32(j)
     return x
+
+
+def octet_capacity():
+    """64-byte tree slots an octet work item holds on the current device."""
+    n = ctypes.c_uint32()
+    rc = lib().jq_batched_oct_capacity(ctypes.byref(n))
+    if rc:
+        raise RuntimeError("jq_batched_oct_capacity: " + sim.lib().jq_strerror(rc).decode())
+    return n.value
 
 
 def to_batched(per_stream):
@@ -194,11 +207,18 @@ class BatchedSim:
         self.eff = getattr(script, "effective_words", None) or \
             script.reg_io_state_size * (2 if script.xprop_enabled else 1)
         self.sig = self.eff * 32
-        # X-capable scripts run in the quad layout: signals [sig/2, sig) are
-        # the X planes of [0, sig/2), which every X partition's offset must say
+        # X-capable scripts run in the quad layout (lane pairs) or the octet
+        # layout (octet items): signals [sig/2, sig) are the X planes of
+        # [0, sig/2), which every X partition's offset must say
         self.x_interleaved = 1 if script.xprop_enabled else 0
         if self.x_interleaved:
             check_x_offsets(script, self.eff // 2)
+        if lanes_per_item == 8:
+            need, cap = self.octet_need(), octet_capacity()
+            if not script.xprop_enabled or lanes % 8 or need > cap:
+                raise ValueError(f"octet items need an X-propagating script, lanes divisible by 8 "
+                                 f"and every partition within {cap} slots (needs {need:#x})")
+            self.x_interleaved = 2
         regions = getattr(script, "input_regions", None)
         if regions is None:
             self.in_sigs = input_words(script) * 32
@@ -226,8 +246,20 @@ class BatchedSim:
         self.record = record
         self.grid = grid
         # lane words per work item: 0 lets the library pick (lane pairs when
-        # lanes is even and they fit), 1 or 2 forces one
+        # lanes is even and they fit), 1, 2 or 8 (octets) forces one
         self.lanes_per_item = lanes_per_item
+
+    def octet_need(self):
+        """The most 64-byte tree slots an octet item needs for any partition
+        of the prepared script (0xffffffff: some partition cannot run as one)."""
+        need = torch.zeros(1, dtype=torch.int32, device=self.device)
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        rc = lib().jq_batched_slot_need(self.ds.blocks_start.data_ptr(), self.prepared.data_ptr(),
+                                        self.ds.num_blocks, self.ds.num_major_stages,
+                                        need.data_ptr(), st)
+        if rc:
+            raise RuntimeError("jq_batched_slot_need: " + sim.lib().jq_strerror(rc).decode())
+        return int(need.cpu().numpy().view(np.uint32)[0])
 
     def _convert(self, fn, src, dst):
         st = torch.cuda.current_stream(self.device).cuda_stream

@@ -66,7 +66,10 @@ struct BatchParams {
   size_t sram_words;
   size_t num_cycles;
   size_t sig_per_snap;      // effective words * 32
-  int xhalf;                // quad layout: signals [V, 2V) are the X of [0, V)
+  int xhalf;                // X interleaved (layout 1 or 2): signals [V, 2V)
+                            // are the X of [0, V)
+  int layout;               // state layout (phys()): 0 pairs, 1 quads, 2 octets
+  uint32_t slot_cap;        // octet items: tree slots of 64 bytes in shared memory
   size_t vsig;              // V: value signals (sig_per_snap / 2 with xhalf)
   uint32_t *state_a, *state_b;  // ping-pong snapshots, interleaved lane pairs (phys())
   const uint32_t *stim;     // [cycle+1][lanes][input_sigs] input values, or null
@@ -167,23 +170,31 @@ __host__ __device__ __forceinline__ uint32_t owned_pos(uint32_t u, int i) {
                         : i < 14 ? 1024 + u + 512 * (i - 12) : i == 14 ? 512 + u : u;
 }
 
-// Word of (lane l, signal s) in the batched state.  Lane pairs are
-// interleaved so the two lane words of a pair (and, with X, their X words)
-// share one 8- or 16-byte access:
-//   quad layout (xhalf, signals [V, 2V) the X of [0, V)):
-//     ((l >> 1) * V + s mod V) * 4 + 2 * (l & 1) + (s >= V)
+// Word of (lane l, signal s) in the batched state, by state layout:
+//   layout 1, lane-pair quads (X interleaved, signals [V, 2V) the X of
+//     [0, V)): ((l >> 1) * V + s mod V) * 4 + 2 * (l & 1) + (s >= V),
 //     i.e. (v_even, x_even, v_odd, x_odd) per lane pair and value signal;
-//   pair layout: ((l >> 1) * sig + s) * 2 + (l & 1).
-__host__ __device__ __forceinline__ size_t phys(int xhalf, size_t vsig, size_t sig, uint32_t l,
+//   layout 2, lane octets (X interleaved): ((l >> 3) * V + s mod V) * 16 +
+//     2 * (l & 7) + (s >= V), i.e. the 64 bytes (v0, x0, ..., v7, x7) of a
+//     signal for 8 lane words (256 streams) are adjacent;
+//   layout 0, lane pairs without X: ((l >> 1) * sig + s) * 2 + (l & 1).
+__host__ __device__ __forceinline__ size_t phys(int layout, size_t vsig, size_t sig, uint32_t l,
                                                 size_t s) {
-  if (xhalf) {
+  if (layout) {
     const bool x = s >= vsig;
-    return ((((size_t)(l >> 1)) * vsig + (x ? s - vsig : s)) << 2) + 2 * (l & 1) + (x ? 1 : 0);
+    const size_t sv = x ? s - vsig : s;
+    if (layout == 2) return ((((size_t)(l >> 3)) * vsig + sv) << 4) + 2 * (l & 7) + (x ? 1 : 0);
+    return ((((size_t)(l >> 1)) * vsig + sv) << 2) + 2 * (l & 1) + (x ? 1 : 0);
   }
   return ((((size_t)(l >> 1)) * sig + s) << 1) + (l & 1);
 }
 __device__ __forceinline__ size_t phys(const BatchParams &P, uint32_t l, size_t s) {
-  return phys(P.xhalf, P.vsig, P.sig_per_snap, l, s);
+  return phys(P.layout, P.vsig, P.sig_per_snap, l, s);
+}
+// log2 of the words one signal of a lane group spans: 1 (pair), 2 (quad),
+// 4 (octet)
+__device__ __forceinline__ uint32_t sig_shift_of(const BatchParams &P) {
+  return P.layout == 2 ? 4u : P.layout == 1 ? 2u : 1u;
 }
 
 constexpr uint32_t MAX_MAJOR_STAGES = 32;  // jq_simulate_batched's limit
@@ -1168,6 +1179,294 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
 #undef JQ_FAIL_IF
 #undef JQ_HOOKS_COMPACT
 
+// Shared memory of an octet item besides the chunks and tree slots: the
+// writeout map (writeout slot -> its first tree slot) and, for setup/hold
+// checks, the OR of each writeout word's clock enables per lane word.
+constexpr uint32_t OCT_AUX_WORDS = 256 + 256 * 8;
+// Global-read slots an octet item loads (16 rounds of 128 slots).
+constexpr uint32_t OCT_MAX_GR = 2048;
+
+// An octet work item: the block's partition list for 8 lane words (256
+// streams) at once, in the octet state layout, so every state access moves a
+// signal's 64 bytes (the 16-byte parts of its four lane pairs) with adjacent
+// threads: thread t handles lane pair k = t & 3 of slot / entry / signal
+// t >> 2 (+ 128 per round).  Every partition must be in the compact form
+// without carries and fit the tree slots (metadata word 127, written by
+// jq_batched_prepare: the slots it needs, or ~0).  A tree slot is 64 bytes:
+// S[4 * slot + k] holds (v, x) of lane words 2k and 2k+1.  Stage regions are
+// never overwritten within a partition, so writeouts are not copied: the
+// writeout map names the tree slots a writeout slot's 32 signals occupy (a
+// hooked 32-slot block of a stage region, or the SRAM stage's staging and
+// read-out slots).
+__device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *aux,
+                          uint32_t *chunks, uint32_t &uses0, uint32_t &uses1,
+                          const uint32_t *script, const uint32_t *in, uint32_t *out, uint32_t og,
+                          uint32_t pid0, bool &failed, unsigned long long &next_ticket,
+                          bool &have_next, bool &pending, unsigned long long &bar_target,
+                          uint32_t cyc) {
+  const int t = threadIdx.x;
+  const uint32_t k = t & 3u, el = (uint32_t)t >> 2;
+  uint32_t *const wo_map = aux;
+  uint32_t *const clk_or = aux + 256;
+  // the octet's words: signal s (value plane) at 16 * (og * V + s)
+  const size_t grp_base = ((size_t)og * P.vsig) << 4;
+  size_t off = 0;
+  uint32_t pid = pid0;
+  for (;;) {
+    __syncthreads();
+    long long t_start = clock64();
+    if (t < 256) sh.meta[t] = __ldg(script + off + t);
+    uint32_t e[16];  // global-read source of slot el + 128 m
+    {
+      const uint32_t *src = P.gr_sources + (size_t)pid * 8192;
+#pragma unroll
+      for (int m = 0; m < 16; ++m) e[m] = __ldg(src + el + 128 * m);
+    }
+    __syncthreads();
+    const uint32_t ns = sh.meta[0];
+    if (!ns) break;
+    const uint32_t is_last = sh.meta[1], num_ios = sh.meta[2], io_off = sh.meta[3];
+    const uint32_t num_srams = sh.meta[4], sram_off = sh.meta[5], R = sh.meta[6];
+    const uint32_t num_dup = sh.meta[7];
+    const bool is_x = sh.meta[8] != 0;
+    const uint32_t need = sh.meta[127];
+    const uint32_t *ch0 = script + off + 256 + 512 * (size_t)R;
+    const bool has_sram = (num_srams | num_dup) != 0;
+    const uint32_t nchunks = ns + (has_sram ? 2 : 1);
+    if (t == 0) {
+      const uint32_t nb = chunk_bytes(sh, 0);
+      mbar_expect_tx(&sh.bar[0], nb);
+      tma_load_1d(chunks, ch0, nb, &sh.bar[0]);
+    }
+    // the deferred wait of the grid barrier ending the previous major stage
+    // (see run_item2); the waiting warps prefetch the commit rows
+    if (pending) {
+      pending = false;
+      const uint32_t *rows = in + grp_base + (((size_t)io_off * 32) << 4);
+      const uint32_t nl = num_ios * 16;  // 128-byte lines
+      if (!grid_wait(P, sh, bar_target, [&](uint32_t i0, uint32_t n) {
+            for (uint32_t l = i0; l < nl; l += n) prefetch_l2(rows + 32 * (size_t)l);
+          })) {
+        failed = true;
+        if (t == 0) mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout);
+        return;
+      }
+      t_start = clock64();
+    }
+    // a partition the octet form cannot run (the host checks the whole
+    // script before choosing this form, so only a malformed launch gets here)
+    if (need > P.slot_cap || !(sh.meta[10] & 1u)) {
+      if (t == 0) {
+        atomicCAS(&g_status[P.slot], 0, JQ_ERR_INVALID_ARG);
+        mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout);
+      }
+      ++uses0;
+      failed = true;
+      return;
+    }
+    if (P.constraints)
+      for (uint32_t i = t; i < num_ios * 8; i += BT) clk_or[i] = 0;
+    // ---- global read: slot el + 128 m, its 16-byte part k, into tree slot
+    // sw(slot) (the prepared stage-0 entries name the swizzled slot, which
+    // stays within the slot's 32-aligned block)
+    if (is_x) {
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const uint32_t ek = e[m];
+        uint4 *dst = &S[4 * sw(el + 128 * m) + k];
+        if (ek < GR_SKIP) {
+          const uint32_t *bp = (ek >> 31) ? out : in;
+          const uint32_t *src = bp + grp_base + ((size_t)(ek & 0x7fffffffu) << 4) + 4 * k;
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+                       : "memory");
+        } else if (ek == GR_EMPTY) {
+          *dst = make_uint4(0, 0, 0, 0);
+        }
+      }
+      asm volatile("cp.async.wait_all;" ::: "memory");
+    } else {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint4 v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const uint32_t ek = e[8 * h + m];
+          v[m] = make_uint4(0, 0, 0, 0);
+          if (ek < GR_SKIP) {
+            const uint32_t *bp = (ek >> 31) ? out : in;
+            v[m] = __ldcg(reinterpret_cast<const uint4 *>(
+                bp + grp_base + ((size_t)(ek & 0x7fffffffu) << 4) + 4 * k));
+            v[m].y = v[m].w = 0u;  // the X planes of a partition without X
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < 8; ++m)
+          if (e[8 * h + m] != GR_SKIP) S[4 * sw(el + 128 * (8 * h + m)) + k] = v[m];
+      }
+    }
+    // writeout slot t's hook (stage << 8 | 32-slot block of the stage's
+    // region); the map entry is set when that stage runs
+    uint32_t my_hook = 0xffffffffu;
+    if ((uint32_t)t < num_ios) {
+      const uint32_t hw = sh.meta[128 + t / 2];
+      my_hook = (t & 1) ? (hw >> 16) : (hw & 0xffffu);
+    }
+    uint32_t reg_end = 0;  // end of the last stage region
+    for (uint32_t ci = 0; ci < nchunks; ++ci) {
+      const uint32_t b = ci & 1;
+      uint32_t *C = chunks + b * STAGE_WORDS;
+      if (ci == 0) __syncthreads();  // global read complete
+      if (t == 0 && ci + 1 < nchunks) {
+        const uint32_t nxt = (!has_sram && ci + 1 == ns) ? ns + 1 : ci + 1;
+        const uint32_t nb = chunk_bytes(sh, nxt);
+        mbar_expect_tx(&sh.bar[b ^ 1], nb);
+        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, nb,
+                    &sh.bar[b ^ 1]);
+      }
+      uint32_t &uses = b ? uses1 : uses0;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.chunk_timeout));
+      ++uses;
+#define JQ_FAIL_IF(cond)                                                    \
+  if (__syncthreads_or(cond)) {                                             \
+    failed = true;                                                          \
+    if (t == 0 && ci + 1 < nchunks)                                         \
+      mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.chunk_timeout); \
+    return;                                                                 \
+  }
+      if (ci < ns) {
+        // ---------------- compact stage ci: entries el + 128 m; its region
+        // follows the previous one, so nothing it reads is overwritten
+        const uint32_t n = ok ? C[0] : 0u, base = ok ? C[1] : 0u;
+        if (ok) {
+          if ((my_hook >> 8) == ci) wo_map[t] = base + 32 * (my_hook & 255u);
+          for (uint32_t i = el; i < n; i += 128) {
+            const uint32_t en = C[4 + i];
+            const uint4 ga = ((en >> 29) & 1u) ? make_uint4(0, 0, 0, 0) : S[4 * (en & 8191u) + k];
+            const uint4 gb =
+                ((en >> 30) & 1u) ? make_uint4(0, 0, 0, 0) : S[4 * ((en >> 13) & 8191u) + k];
+            S[4 * (base + i) + k] = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u),
+                                          0u - ((en >> 28) & 1u));
+          }
+          reg_end = base + n;
+        }
+        JQ_FAIL_IF(!ok)
+      } else if (has_sram && ci == ns) {
+        // ---------------- SRAM & duplicate permutation + SRAM ports: staged
+        // words past the last region, then 32 read-out slots per SRAM
+        JQ_FAIL_IF(!ok)
+        const uint32_t st0 = (reg_end + 31) & ~31u;
+        const uint32_t nq = (num_srams * 4 + num_dup) * 32;
+        const uint32_t ro = st0 + nq;
+        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
+        for (uint32_t q = el; q < nq; q += 128) {
+          const uint32_t p = perm_lin(C, q);
+          const uint4 w = S[4 * (wo_map[p >> 5] + (p & 31u)) + k];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q);
+          S[4 * (st0 + q) + k] = make_uint4((w.x & ~set0) ^ inv, is_x ? (w.y & ~set0) : 0u,
+                                            (w.z & ~set0) ^ inv, is_x ? (w.w & ~set0) : 0u);
+        }
+        __syncthreads();
+        // one warp per (SRAM, lane word), lane = stream; a slot's word of
+        // lane word lw (value, X) is word 2 lw (+1) of its 16
+        uint32_t *Sw = reinterpret_cast<uint32_t *>(S);
+        const int warp = t >> 5, ln = t & 31;
+        for (uint32_t ih = warp; ih < num_srams * 8; ih += BT / 32) {
+          const uint32_t i = ih >> 3, lw = ih & 7u;
+          const uint32_t *Aw = Sw + 16 * (size_t)(st0 + 128 * i) + 2 * lw;
+          const uint32_t addr = warp_transpose32(Aw[16 * ln]);
+          const uint32_t ra = addr & 0xffffu, wa = addr >> 16;
+          const uint32_t en = warp_transpose32(Aw[16 * (32 + ln)]);
+          const uint32_t data = warp_transpose32(Aw[16 * (64 + ln)]);
+          const uint32_t datax = warp_transpose32(Aw[16 * (64 + ln) + 1]);
+          const size_t stream = (size_t)(8 * og + lw) * 32 + ln;
+          uint32_t *ram = P.sram + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS;
+          const uint32_t r = ldcg(ram + ra), w0 = ldcg(ram + wa);
+          uint32_t rx = 0, w0x = 0;
+          const bool hx = is_x && P.sram_x != nullptr;
+          uint32_t *ramx = hx ? P.sram_x + stream * P.sram_words + sram_off + (size_t)i * SRAM_WORDS
+                              : nullptr;
+          if (hx) {
+            rx = ldcg(ramx + ra);
+            w0x = ldcg(ramx + wa);
+          }
+          ram[wa] = (w0 & ~en) | (data & en);
+          if (hx) ramx[wa] = (w0x & ~en) | (datax & en);
+          const uint32_t word = warp_transpose32(r), wordx = warp_transpose32(rx);
+          *reinterpret_cast<uint2 *>(Sw + 16 * (size_t)(ro + 32 * i + ln) + 2 * lw) =
+              make_uint2(word, is_x ? wordx : 0u);
+        }
+        // duplicates are the staged words themselves; SRAM read-outs follow
+        if ((uint32_t)t < num_dup) wo_map[num_ios - num_srams - num_dup + t] = st0 + 32 * (num_srams * 4 + t);
+        if ((uint32_t)t < num_srams) wo_map[num_ios - num_srams + t] = ro + 32 * t;
+        __syncthreads();
+      } else {
+        // ---------------- clock-enable permutation and commit: signal el +
+        // 128 m, lane pair k; a warp's 8 signals lie in one state word
+        JQ_FAIL_IF(!ok)
+        if (t == 0 && is_last && sh.dyn) {
+          next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
+          have_next = true;
+        }
+        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
+        const uint32_t nq = num_ios * 32;
+        for (uint32_t q = el; q < nq; q += 128) {  // warp-uniform bound
+          const uint32_t p = perm_lin(C, q);
+          const uint4 src = S[4 * (wo_map[p >> 5] + (p & 31u)) + k];
+          const uint4 me = S[4 * (wo_map[q >> 5] + (q & 31u)) + k];
+          const uint4 fl = F4[q >> 5];
+          const uint32_t inv = bitmask(fl.x, q), set0 = bitmask(fl.y, q), dinv = bitmask(fl.z, q);
+          const uint32_t cp0 = (src.x & ~set0) ^ inv, cp1 = (src.z & ~set0) ^ inv;
+          if (P.constraints) {
+            atomicOr(&clk_or[(q >> 5) * 8 + 2 * k], cp0);
+            atomicOr(&clk_or[(q >> 5) * 8 + 2 * k + 1], cp1);
+          }
+          const size_t w = grp_base + ((((size_t)io_off * 32 + q)) << 4) + 4 * k;
+          uint32_t o0 = 0, o1 = 0, ox0 = 0, ox1 = 0;  // old v0, v1, x0, x1
+          if (__any_sync(0xffffffffu, (cp0 & cp1) != 0xffffffffu)) {
+            const uint4 o = __ldcg(reinterpret_cast<const uint4 *>(in + w));
+            o0 = o.x;
+            ox0 = o.y;
+            o1 = o.z;
+            ox1 = o.w;
+          }
+          const uint32_t n0 = (o0 & ~cp0) | ((me.x ^ dinv) & cp0);
+          const uint32_t n1 = (o1 & ~cp1) | ((me.z ^ dinv) & cp1);
+          if (is_x) {
+            const uint32_t cx0 = src.y & ~set0, cx1 = src.w & ~set0;
+            *reinterpret_cast<uint4 *>(out + w) =
+                make_uint4(n0, (ox0 & ~cp0 & ~cx0) | (me.y & cp0 & ~cx0) | cx0, n1,
+                           (ox1 & ~cp1 & ~cx1) | (me.w & cp1 & ~cx1) | cx1);
+          } else {  // values only; the X words keep theirs
+            out[w] = n0;
+            out[w + 2] = n1;
+          }
+        }
+        if (P.constraints) {
+          // setup/hold checks per state word, a warp per word (check_word
+          // per two lane words)
+          __syncthreads();
+          for (uint32_t j = (uint32_t)t >> 5; j < num_ios; j += BT / 32) {
+#pragma unroll 1
+            for (uint32_t kk = 0; kk < 4; ++kk)
+              check_word(P, io_off + j, clk_or[8 * j + 2 * kk], 8 * og + 2 * kk,
+                         clk_or[8 * j + 2 * kk + 1], 8 * og + 2 * kk + 1, P.first_cycle + cyc,
+                         cyc == 0);
+          }
+        }
+      }
+#undef JQ_FAIL_IF
+    }
+    off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
+    if (P.part_cycles) {
+      __syncthreads();
+      if (t == 0) atomicAdd(&P.part_cycles[pid], (unsigned long long)(clock64() - t_start));
+    }
+    ++pid;
+    if (is_last) break;
+  }
+}
+
 
 // L2 prefetch of what the CTA's item of major stage ms reads first, when
 // that stage assigns items statically (at most one per CTA): the global-read
@@ -1200,7 +1499,8 @@ __device__ void prefetch_item_l2(const BatchParams &P, const Shared &sh, unsigne
   const uint32_t per = P.lanes / NL;
   const uint32_t lane0 = NL * (blockIdx.x % per);
   const size_t w0 = phys(P, lane0 & ~1u, (size_t)sh.st_io[ms] * 32);
-  const uint32_t rows = sh.st_nio[ms] * (P.xhalf ? 4 : 2);  // 32 signals x 16 or 8 bytes
+  // 128-byte lines: 32 signals of 2^shift words each per writeout slot
+  const uint32_t rows = sh.st_nio[ms] << sig_shift_of(P);
   for (uint32_t l = i0; l < GR_LINES + script_lines + rows; l += n) {
     if (l < GR_LINES)
       prefetch_l2(gr + 32 * l);
@@ -1222,8 +1522,8 @@ __device__ void prefetch_global_read_l2(const BatchParams &P, const Shared &sh, 
   const uint32_t *row = P.gr_sources + (size_t)sh.st_pid[ms] * 8192;
   const uint32_t per = P.lanes / NL;
   const uint32_t lane0 = NL * (blockIdx.x % per);
-  const size_t pb = phys(P, lane0 & ~1u, 0);  // the lane pair's word of signal 0
-  const uint32_t sh2 = P.xhalf ? 2 : 1;
+  const size_t pb = phys(P, lane0 & ~1u, 0);  // the lane group's word of signal 0
+  const uint32_t sh2 = sig_shift_of(P);
   constexpr int K = 18;  // 18 * 480 >= 8192 slots: one round of row loads
   for (uint32_t q0 = i0; q0 < 8192; q0 += K * n) {
     uint32_t ev[K];
@@ -1235,24 +1535,28 @@ __device__ void prefetch_global_read_l2(const BatchParams &P, const Shared &sh, 
   }
 }
 
-// NL lane words per work item (1, or 2 for run_item2); DS only with NL = 1.
+// NL lane words per work item (1, 2 for run_item2, 8 for run_item8); DS
+// only with NL = 1.
 template <bool DS, int NL>
 __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
-  static_assert(NL == 1 || (NL == 2 && !DS), "lane pairs use a single tree buffer");
+  static_assert(NL == 1 || ((NL == 2 || NL == 8) && !DS), "only single lanes double-buffer");
   extern __shared__ __align__(128) uint8_t dyn[];
   __shared__ Shared sh;
-  constexpr size_t WB = NL == 2 ? 16 : 8;  // bytes per tree / writeout word
+  constexpr size_t WB = NL == 2 ? 16 : 8;  // bytes per tree / writeout word (NL 1, 2)
   uint32_t *chunks = reinterpret_cast<uint32_t *>(dyn);               // 2 x 20 KB
-  uint8_t *S = dyn + 2 * CHUNK_BYTES;                                  // (1 or 2) x 8192 words
-  uint8_t *WO = S + (DS ? 2 : 1) * 8192 * WB;                          // wo_slots*32 words
+  // NL 1, 2: tree state ((1 or 2) x 8192 words), then the writeouts
+  // (wo_slots * 32 words); NL 8: the writeout map and clock-enable ORs, then
+  // slot_cap tree slots of 64 bytes
+  uint8_t *S = dyn + 2 * CHUNK_BYTES + (NL == 8 ? OCT_AUX_WORDS * 4 : 0);
+  uint8_t *WO = NL == 8 ? dyn + 2 * CHUNK_BYTES : S + (DS ? 2 : 1) * 8192 * WB;
   const int t = threadIdx.x;
   if (t == 0) {
     mbar_init(&sh.bar[0], 1);
     mbar_init(&sh.bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (uint32_t q = t; q < P.wo_slots * 32 * (uint32_t)(WB / 4); q += BT)
-    reinterpret_cast<uint32_t *>(WO)[q] = 0;
+  const uint32_t wo_words = NL == 8 ? OCT_AUX_WORDS : P.wo_slots * 32 * (uint32_t)(WB / 4);
+  for (uint32_t q = t; q < wo_words; q += BT) reinterpret_cast<uint32_t *>(WO)[q] = 0;
   // item table: thread ms resolves major stage ms
   if (t == 0) sh.script_words = P.blocks_start[(size_t)P.num_major_stages * P.num_blocks];
   if ((unsigned)t < P.num_major_stages) {
@@ -1281,12 +1585,12 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
     sh.st_io[t] = io;
   }
   __syncthreads();
-  // Lane-pair groups: with lane pairs and one item per CTA in every major
-  // stage, CTA i always runs lane pair i % per, and the CTAs of one lane
-  // pair (which alone read and write that pair's state words, SRAM rows,
+  // Lane groups: with lane pairs or octets and one item per CTA in every
+  // major stage, CTA i always runs lane group i % per, and the CTAs of one
+  // group (which alone read and write that group's state words, SRAM rows,
   // stimulus and outputs) form their own barrier group.
   const uint32_t per_lp = P.lanes / NL;
-  bool grouped = NL == 2 && per_lp > 1 && per_lp <= MAX_GROUPS && gridDim.x >= per_lp;
+  bool grouped = NL >= 2 && per_lp > 1 && per_lp <= MAX_GROUPS && gridDim.x >= per_lp;
   for (unsigned ms = 0; ms < P.num_major_stages; ++ms) grouped &= sh.st_items[ms] <= gridDim.x;
   const uint32_t grp = grouped ? blockIdx.x % per_lp : 0;         // lane pair of this CTA
   const uint32_t grp_rank = grouped ? blockIdx.x / per_lp : blockIdx.x;
@@ -1295,8 +1599,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
     sh.bar_count = grouped ? &g_bgroup[(size_t)P.slot * MAX_GROUPS + grp] : &g_bcount[P.slot];
     sh.bar_size = grp_ctas;
   }
-  // lanes this CTA copies stimulus for and records: its lane pair, or all
-  const uint32_t lane_lo = grouped ? 2 * grp : 0, lane_n = grouped ? 2 : P.lanes;
+  // lanes this CTA copies stimulus for and records: its lane group, or all
+  const uint32_t lane_lo = grouped ? NL * grp : 0, lane_n = grouped ? NL : P.lanes;
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;
   bool failed = false;
@@ -1306,7 +1610,7 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
   const size_t snap = P.sig_per_snap * P.lanes;  // lane-major record snapshot
   // Lane-pair items take over the barrier that ends the previous major
   // stage (see run_item2); `pending` marks one owed.
-  constexpr bool DEFER = NL == 2;
+  constexpr bool DEFER = NL >= 2;
   bool pending = false;
   auto no_prefetch = [](uint32_t, uint32_t) {};
 
@@ -1380,7 +1684,11 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
           if (t < 256) prefetch_l2(nrow + 32 * t);
           else if (t < 256 + 48) prefetch_l2(nscr + 32 * (t - 256));  // metadata, chunk 0 head
         }
-        if constexpr (NL == 2)
+        if constexpr (NL == 8)
+          run_item8(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint32_t *>(WO), chunks,
+                    uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
+                    pending, bar_target, (uint32_t)c);
+        else if constexpr (NL == 2)
           run_item2(P, sh, reinterpret_cast<uint4 *>(S), reinterpret_cast<uint4 *>(WO), chunks,
                     uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
                     pending, bar_target, (uint32_t)c);
@@ -1388,8 +1696,8 @@ __global__ void __launch_bounds__(BT, 1) jq_batched_kernel(BatchParams P) {
           run_item<DS>(P, sh, reinterpret_cast<uint2 *>(S), reinterpret_cast<uint2 *>(WO), chunks,
                        uses0, uses1, script, in, out, lane, pid0, failed, next_ticket, have_next,
                        (uint32_t)c);
-        if (failed) {
-          if (t == 0) atomicExch(&g_status[P.slot], JQ_ERR_BARRIER_TIMEOUT);
+        if (failed) {  // the first error recorded stays
+          if (t == 0) atomicCAS(&g_status[P.slot], 0, JQ_ERR_BARRIER_TIMEOUT);
           return;
         }
       }
@@ -1740,8 +2048,8 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     // when the value is to be inverted (direct variant), REF_ZERO for the
     // constant 0 (and for positions nothing reads), REF_ONE for constant 1.
     constexpr uint32_t REF_ZERO = 0xffffu, REF_ONE = 0xfffeu;
+    uint32_t next_base = gr_top;  // end of the stage regions (direct variant)
     if (compact) {
-      uint32_t next_base = gr_top;
       for (uint32_t ci = 0; ci < ns; ++ci) {
         const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
         uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
@@ -1916,6 +2224,28 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
         __syncthreads();
       }
     }
+    // Metadata word 127: the 64-byte tree slots an octet item needs for this
+    // partition (run_item8: global-read slots, stage regions, then the SRAM
+    // stage's staged words and read-outs), or ~0 when the octet form cannot
+    // run it: it needs the compact form without carries (regions never
+    // overwritten, so writeouts name tree slots), at most OCT_MAX_GR
+    // global-read slots, and a hook for every writeout slot but the SRAM and
+    // duplicate ones.
+    {
+      const uint32_t nsr = src[off + 4], ndup = src[off + 7];
+      bool hooked = true;
+      for (uint32_t j = t; j < nio; j += BT) {
+        const uint32_t hw = src[off + 128 + j / 2];
+        const uint32_t hook = (j & 1) ? (hw >> 16) : (hw & 0xffffu);
+        if (j + nsr + ndup < nio && (hook >> 8) >= ns) hooked = false;
+      }
+      hooked = !__syncthreads_or(!hooked);
+      if (t == 0) {
+        const bool oct = compact && direct && hooked && n_gr <= OCT_MAX_GR;
+        dst[off + 127] = oct ? ((next_base + 31) & ~31u) + (nsr * 4 + ndup) * 32 + nsr * 32
+                             : 0xffffffffu;
+      }
+    }
     if (t == 0) {
       dst[off + 10] = compact ? 1u : 0u;
       if (compact) dst[off + 11 + ns] = dst[off + 12 + ns] = 0;  // SRAM, commit: whole
@@ -1931,6 +2261,25 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
     ++pid;
     if (is_last) break;
   }
+}
+
+// Largest octet slot need (metadata word 127 of the prepared script) over
+// each entry's partition list, into *need by atomic maximum.
+__global__ void jq_batched_need_kernel(const size_t *blocks_start, const uint32_t *prep,
+                                       uint32_t *need, unsigned entries) {
+  const unsigned e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= entries) return;
+  size_t off = blocks_start[e];
+  uint32_t m = 0;
+  for (;;) {
+    const uint32_t ns = prep[off];
+    if (!ns) break;
+    const uint32_t w = prep[off + 127];
+    m = w > m ? w : m;
+    if (prep[off + 1]) break;
+    off += 256 + 512 * (size_t)prep[off + 6] + STAGE_WORDS * ((size_t)ns + 2);
+  }
+  if (m) atomicMax(need, m);
 }
 
 // Number of partitions in each (major stage, block) entry's list.
@@ -1956,11 +2305,11 @@ using namespace jqk;
 
 // Lane-major [lane][signal] snapshot <-> the interleaved batched state.
 __global__ void jq_batched_pack_kernel(const uint32_t *lm, uint32_t *st, uint32_t lanes,
-                                       size_t sig, int xhalf, int unpack) {
+                                       size_t sig, int layout, int unpack) {
   const size_t n = (size_t)lanes * sig;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const size_t w = phys(xhalf, sig / 2, sig, (uint32_t)(q / sig), q % sig);
+    const size_t w = phys(layout, sig / 2, sig, (uint32_t)(q / sig), q % sig);
     if (unpack)
       st[q] = lm[w];  // st: lane-major output, lm: batched input
     else
@@ -1981,34 +2330,57 @@ extern "C" {
 
 // Kernel variant: lane words per work item and tree-state buffering.
 struct Variant {
-  int nl;   // 1 or 2 lane words per item
+  int nl;   // 1, 2 or 8 lane words per item
   bool ds;  // double-buffered tree state (nl == 1 only)
 };
 
 static const void *variant_fn(Variant v) {
+  if (v.nl == 8) return (const void *)jq_batched_kernel<false, 8>;
   if (v.nl == 2) return (const void *)jq_batched_kernel<false, 2>;
   return v.ds ? (const void *)jq_batched_kernel<true, 1> : (const void *)jq_batched_kernel<false, 1>;
 }
 
+// Opt-in shared memory per CTA left for the dynamic part of variant v.
+static size_t dyn_smem_limit(Variant v) {
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, variant_fn(v)) != cudaSuccess || (size_t)optin < fa.sharedSizeBytes)
+    return 0;
+  return (size_t)optin - fa.sharedSizeBytes;
+}
+
+// 64-byte tree slots of an octet item: what the opt-in shared memory leaves
+// after the chunk buffers and the writeout map.
+static uint32_t oct_slot_capacity() {
+  const size_t lim = dyn_smem_limit(Variant{8, false});
+  const size_t fixed = 2 * (size_t)CHUNK_BYTES + OCT_AUX_WORDS * 4;
+  if (lim <= fixed) return 0;
+  const size_t n = (lim - fixed) / 64;
+  return (uint32_t)(n < 8192 ? n : 8192);
+}
+
 static size_t smem_layout_bytes(uint32_t wo_slots, Variant v) {
+  if (v.nl == 8) return 2 * (size_t)CHUNK_BYTES + OCT_AUX_WORDS * 4 + (size_t)oct_slot_capacity() * 64;
   const size_t wb = v.nl == 2 ? 16 : 8;
   return 2 * (size_t)CHUNK_BYTES + (v.ds ? 2 : 1) * 8192 * wb + (size_t)wo_slots * 32 * wb;
 }
 
 static bool variant_fits(uint32_t wo_slots, Variant v) {
-  int dev = 0, optin = 0;
-  cudaFuncAttributes fa;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-      cudaFuncGetAttributes(&fa, variant_fn(v)) != cudaSuccess)
-    return false;
-  return smem_layout_bytes(wo_slots, v) + fa.sharedSizeBytes <= (size_t)optin;
+  return smem_layout_bytes(wo_slots, v) <= dyn_smem_limit(v);
 }
 
 // want_nl 0 = automatic: lane pairs when the lane count is even and their
 // shared memory fits, else single lanes, double-buffered when that fits.
-// nl = 0 in the result: the requested variant is not possible.
-static Variant pick_variant(uint32_t wo_slots, uint32_t lanes, uint32_t want_nl) {
+// The octet layout (2) runs octet items only.  nl = 0 in the result: the
+// requested variant is not possible.
+static Variant pick_variant(uint32_t wo_slots, uint32_t lanes, uint32_t want_nl, int layout) {
+  if (layout == 2)
+    return (want_nl == 0 || want_nl == 8) && lanes % 8 == 0 && oct_slot_capacity() > 0
+               ? Variant{8, false}
+               : Variant{0, false};
+  if (want_nl == 8) return Variant{0, false};
   if (want_nl != 1 && lanes % 2 == 0 && variant_fits(wo_slots, Variant{2, false}))
     return Variant{2, false};
   if (want_nl == 2) return Variant{0, false};
@@ -2016,7 +2388,7 @@ static Variant pick_variant(uint32_t wo_slots, uint32_t lanes, uint32_t want_nl)
 }
 
 int jq_batched_smem_bytes(uint32_t wo_slots) {
-  return (int)smem_layout_bytes(wo_slots, pick_variant(wo_slots, 1, 1));
+  return (int)smem_layout_bytes(wo_slots, pick_variant(wo_slots, 1, 1, 0));
 }
 
 static int variant_max_blocks(int device, uint32_t wo_slots, Variant v, size_t *max_blocks) {
@@ -2034,7 +2406,13 @@ static int variant_max_blocks(int device, uint32_t wo_slots, Variant v, size_t *
 
 int jq_batched_max_blocks(int device, uint32_t wo_slots, size_t *max_blocks) {
   // every variant runs one CTA per SM
-  return variant_max_blocks(device, wo_slots, pick_variant(wo_slots, 1, 1), max_blocks);
+  return variant_max_blocks(device, wo_slots, pick_variant(wo_slots, 1, 1, 0), max_blocks);
+}
+
+int jq_batched_oct_capacity(uint32_t *slots) {
+  if (!slots) return JQ_ERR_INVALID_ARG;
+  *slots = oct_slot_capacity();
+  return JQ_OK;
 }
 
 size_t jq_batched_gr_words(size_t num_partitions) { return (num_partitions + 1) * 8192; }
@@ -2045,12 +2423,13 @@ size_t jq_batched_state_words(uint32_t lanes, size_t signals) {
 
 static int pack_launch(const uint32_t *src, uint32_t *dst, uint32_t lanes, size_t signals,
                        int32_t x_interleaved, int unpack, void *stream) {
-  if (!src || !dst || lanes == 0 || signals == 0 || (x_interleaved && (signals & 1)))
+  if (!src || !dst || lanes == 0 || signals == 0 || x_interleaved < 0 || x_interleaved > 2 ||
+      (x_interleaved && (signals & 1)) || (x_interleaved == 2 && lanes % 8))
     return JQ_ERR_INVALID_ARG;
   const size_t n = (size_t)lanes * signals;
   const unsigned grid = (unsigned)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
   jq_batched_pack_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(src, dst, lanes, signals,
-                                                                   x_interleaved != 0, unpack);
+                                                                   x_interleaved, unpack);
   return cudaGetLastError() == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
 }
 
@@ -2116,6 +2495,18 @@ int jq_batched_prepare(const size_t *blocks_start, const uint32_t *blocks_data,
   return rc;
 }
 
+int jq_batched_slot_need(const size_t *blocks_start, const uint32_t *prepared, size_t num_blocks,
+                         size_t num_major_stages, uint32_t *need, void *stream) {
+  if (!blocks_start || !prepared || !need || num_blocks == 0 || num_major_stages == 0)
+    return JQ_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t entries = num_blocks * num_major_stages;
+  if (cudaMemsetAsync(need, 0, sizeof(uint32_t), st) != cudaSuccess) return JQ_ERR_CUDA;
+  jq_batched_need_kernel<<<(unsigned)((entries + 255) / 256), 256, 0, st>>>(
+      blocks_start, prepared, need, (unsigned)entries);
+  return cudaGetLastError() == cudaSuccess ? JQ_OK : JQ_ERR_LAUNCH;
+}
+
 int jq_simulate_batched(const jq_batch_args *a) {
   if (!a || a->lanes == 0 || a->num_blocks == 0 || a->num_major_stages == 0 ||
       a->num_major_stages > 32 || !a->state_a || !a->state_b || a->wo_slots > 256 ||
@@ -2125,8 +2516,10 @@ int jq_simulate_batched(const jq_batch_args *a) {
   int dev = 0;
   cudaGetDevice(&dev);
   const uint32_t wo_slots = a->wo_slots ? a->wo_slots : 256;
-  if (a->lanes_per_item > 2) return JQ_ERR_INVALID_ARG;
-  const Variant v = pick_variant(wo_slots, a->lanes, a->lanes_per_item);
+  if ((a->lanes_per_item > 2 && a->lanes_per_item != 8) || a->x_interleaved < 0 ||
+      a->x_interleaved > 2)
+    return JQ_ERR_INVALID_ARG;
+  const Variant v = pick_variant(wo_slots, a->lanes, a->lanes_per_item, a->x_interleaved);
   if (v.nl == 0) return JQ_ERR_INVALID_ARG;
   size_t maxg = 0;
   if (variant_max_blocks(dev, wo_slots, v, &maxg) != JQ_OK || maxg == 0) return JQ_ERR_LAUNCH;
@@ -2145,6 +2538,8 @@ int jq_simulate_batched(const jq_batch_args *a) {
   P.sig_per_snap = a->signals_per_snapshot;
   if (a->x_interleaved && (P.sig_per_snap & 1)) return JQ_ERR_INVALID_ARG;
   P.xhalf = a->x_interleaved != 0;
+  P.layout = a->x_interleaved;
+  P.slot_cap = v.nl == 8 ? oct_slot_capacity() : 0;
   P.vsig = P.xhalf ? P.sig_per_snap / 2 : P.sig_per_snap;
   P.state_a = a->state_a;
   P.state_b = a->state_b;

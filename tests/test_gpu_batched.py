@@ -49,6 +49,31 @@ def test_batched_balanced_partitions_match_oracle(kind, nb, split, parts, lanes,
     check_batched(kind, s, lanes, None, 2, grid)
 
 
+SPLIT4 = tuple(range(4, 80, 4))  # the benchmark's level split (20 major stages)
+
+
+@pytest.mark.parametrize("kind,nb,split,parts,lanes,grid", [
+    ("soc_mini", 148, SPLIT4, 37, 8, 0),     # one octet item per CTA per stage
+    ("soc_mini", 148, SPLIT4, 37, 16, 0),    # two octet groups, own barriers
+    ("soc_mini", 148, SPLIT4, 37, 8, 7),     # tickets
+    ("sram", 16, (8,), 16, 8, 0),            # SRAM ports and duplicates
+])
+def test_batched_octet_items_match_oracle(kind, nb, split, parts, lanes, grid):
+    """Octet work items (8 lane words, the octet state layout, writeouts
+    named in the tree slots) on balanced flat partitions, every stream
+    against the oracle."""
+    s = cases.script(kind, nb, split, xprop=True, target_parts=parts)
+    check_batched(kind, s, lanes, None, 8, grid)
+
+
+def test_octet_items_refuse_a_script_they_cannot_run():
+    """Octet items need the compact form: a script in the tree form (deep
+    boomerang stages) is refused on the host, before any launch."""
+    s = cases.script("sram", 16, (8,), xprop=True)
+    with pytest.raises(ValueError):
+        batched.BatchedSim(s, 8, lanes_per_item=8)
+
+
 class BatchedCase:
     """A batched run prepared on the device with its per-stream oracle
     results: launch() issues it (on any stream), verify() checks every
@@ -203,7 +228,7 @@ def test_multi_design_single_launch_matches_oracle():
 
 @pytest.mark.parametrize("xprop,lanes,per_item,parts", [(False, 2, 2, 0), (True, 2, 2, 0),
                                                          (True, 1, 1, 0), (True, 2, 2, 4),
-                                                         (True, 4, 2, 4)])
+                                                         (True, 4, 2, 4), (True, 8, 8, 16)])
 def test_batched_setup_hold_events_match_oracle_per_stream(xprop, lanes, per_item, parts):
     """Setup/hold checks in the batched interpreter, two launch windows of 12
     cycles: every stream's snapshots, and the multiset of (stream, event)
