@@ -201,18 +201,31 @@ def learned_model():
     return costmodel.packed_from_file(MODEL_PATH)
 
 
-def learned_wins():
+def learned_wins(parts_per_stage, lanes_per_item):
     """Whether the committed training summary shows the learned cut beating
-    the heuristic on this workload's own design (the 2M-gate SoC, 37
-    partitions per stage, 256 streams), with the learned run bit-exact
-    against the heuristic one.  The benchmark uses the learned cut by
-    default only then."""
+    the heuristic on this workload's own design (the 2M-gate SoC, 256
+    streams) in the same configuration (partitions per major stage, lane
+    words per work item), with the learned run bit-exact against the
+    heuristic one.  The benchmark uses the learned cut by default only
+    then."""
     p = os.path.splitext(MODEL_PATH)[0] + ".json"
     if not os.path.exists(MODEL_PATH) or not os.path.exists(p):
         return False
     with open(p) as f:
         ev = json.load(f).get("eval_soc2m", {})
-    return bool(ev.get("bit_exact_vs_heuristic")) and ev.get("gain", 0.0) > 1.0
+    return (bool(ev.get("bit_exact_vs_heuristic")) and ev.get("gain", 0.0) > 1.0
+            and ev.get("parts_per_stage") == parts_per_stage
+            and ev.get("lanes_per_item", 2) == lanes_per_item)
+
+
+def default_batched_script(d, blocks=148, lanes=8, per_item=8, learned="auto"):
+    """(script, lanes per item) exactly as the batched mode builds them with
+    these options: balanced partitions, one round of work items per major
+    stage, the learned cut when `learned` says so."""
+    per_stage = blocks // max(1, lanes // per_item)
+    use = learned == "on" or (learned == "auto" and learned_wins(per_stage, per_item))
+    return build_script(d, blocks, cost_model=learned_model() if use else None,
+                        target_parts=per_stage), per_item
 
 
 def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0):
@@ -233,7 +246,9 @@ def algorithmic_bytes_per_cycle(s, streams=1, arrivals=False, bit_sliced=False):
     """(script bytes, state bytes) one simulated cycle must move.
 
     Script: every word of the script (FlattenedScriptV1, empty-block dummies
-    included), read once per cycle however many streams share it.
+    included), read once per cycle however many streams share it.  (The
+    batched modes report the prepared script's streamed bytes instead:
+    prepared_script_bytes.)
     State, per partition (x = 1 on X-capable partitions): the global-read
     bits, the IO words read (old value) and written, the SRAM words (read,
     old word at the write address, write), each with its X copy.
@@ -269,6 +284,37 @@ def algorithmic_bytes_per_cycle(s, streams=1, arrivals=False, bit_sliced=False):
             if last:
                 break
     return 4 * script_words, 4 * (gr + io + sr)
+
+
+def prepared_script_bytes(B):
+    """Script bytes the batched kernel must stream per simulated cycle, once
+    per partition (all streams share them): the metadata (1 KB), a 4-byte
+    source entry per global-read slot it loads, and the copied part of each
+    chunk of the prepared script (the used head of a compact chunk, the whole
+    20 KB chunk otherwise).  The rest of FlattenedScriptV1's fixed-size
+    chunks is padding the kernel never reads."""
+    bd = B.prepared.cpu().numpy().view(np.uint32)
+    bs = np.asarray(B.script.blocks_start, np.int64)
+    total = 0
+    for e in range(bs.size - 1):
+        off = int(bs[e])
+        while True:
+            ns = int(bd[off])
+            if ns == 0:
+                break
+            R, compact = int(bd[off + 6]), bool(bd[off + 10] & 1)
+            chunks = list(range(ns)) + ([ns] if (bd[off + 4] | bd[off + 7]) else []) + [ns + 1]
+            total += 1024
+            for k in chunks:
+                b = int(bd[off + 11 + k]) if compact and k < 116 else 0
+                total += b or 5120 * 4
+            last = int(bd[off + 1])
+            off += 256 + 512 * R + 5120 * (ns + 2)
+            if last:
+                break
+    gr = B.gr_sources.view(-1, 8192)[:B.num_partitions]
+    total += 4 * int(((gr != -1) & (gr != -2)).sum().item())  # GR_EMPTY, GR_SKIP
+    return total
 
 
 def stimulus_window(s, d, first_cycle, cycles, seed):
@@ -437,10 +483,11 @@ def run_mine_batched(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
-    use_learned = args.learned == "on" or (args.learned == "auto" and learned_wins())
-    model = learned_model() if use_learned else None
     per_stage = args.blocks // max(1, args.lanes // args.per_item)  # one round of items
-    s = build_script(d, args.blocks, cost_model=model, target_parts=per_stage)
+    use_learned = args.learned == "on" or (args.learned == "auto" and
+                                           learned_wins(per_stage, args.per_item))
+    model = learned_model() if use_learned else None
+    s, _ = default_batched_script(d, args.blocks, args.lanes, args.per_item, args.learned)
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
@@ -499,14 +546,16 @@ def run_mine_batched(args, rank, world):
         at_end = check.capture()
         parity = (check.replay(at_start, at_mid, args.steps, wave_dev_region)
                   and check.replay(at_mid, at_end, args.steps, wave_pin.to(dev)))
-    script_b, state_b = algorithmic_bytes_per_cycle(s, streams=streams, bit_sliced=True)
+    format_b, state_b = algorithmic_bytes_per_cycle(s, streams=streams, bit_sliced=True)
+    script_b = prepared_script_bytes(B)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams,
                 clocks=ck.summary(), bytes_per_cycle=script_b + state_b, script_bytes=script_b,
                 kernel_ms=dev_ms / args.steps, h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4,
                 launches_per_step=2, parity=parity,
                 traffic_per_cycle=measured_traffic_per_cycle() if args.clusters == 512 else None,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
-                            script_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
+                            script_mb_per_cycle=format_b / 1e6,
+                            script_read_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
                             lanes_per_item=args.per_item,
                             partitioner="balanced: at most %d per major stage%s"
@@ -543,13 +592,14 @@ def run_mine_timed(args, rank, world):
     from jacquard_b200 import batched, state, timing
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    d, s, cons = timed_design(args, rank, args.blocks, args.blocks // max(1, args.lanes // 2))
+    d, s, cons = timed_design(args, rank, args.blocks,
+                              args.blocks // max(1, args.lanes // args.per_item))
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
     assert W % 2 == 0
     po_sig = state.po_positions(s, d)
-    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig)
+    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig, lanes_per_item=args.per_item)
     cap = args.event_capacity
     tm = batched.Timing(s, cons, cap, device=dev)
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
@@ -613,13 +663,15 @@ def run_mine_timed(args, rank, world):
     timed_region_edge(world)
     e2e_ms = (time.perf_counter() - w0) * 1e3
     assert B.status(stream) == 0
-    script_b, state_b = algorithmic_bytes_per_cycle(s, streams=streams, bit_sliced=True)
+    format_b, state_b = algorithmic_bytes_per_cycle(s, streams=streams, bit_sliced=True)
+    script_b = prepared_script_bytes(B)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams, clocks=ck.summary(),
                 bytes_per_cycle=script_b + state_b, script_bytes=script_b,
                 kernel_ms=dev_ms / args.steps,
                 h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4, launches_per_step=2,
                 design=dict(ands=int(d.num_and), dffs=int(d.num_dffs), partitions=s.num_partitions,
-                            script_mb_per_cycle=script_b / 1e6, rio=rio,
+                            script_mb_per_cycle=format_b / 1e6,
+                            script_read_mb_per_cycle=script_b / 1e6, rio=rio,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
                             setup_violations=stats["setup_violations"],
                             hold_violations=stats["hold_violations"],
@@ -812,10 +864,11 @@ def run_mine_multi(args, rank, world):
     del g
     streams = 32 * lanes * len(scripts)
     per = [algorithmic_bytes_per_cycle(s, streams=32 * lanes, bit_sliced=True) for s in scripts]
-    bytes_per_cycle = sum(p[0] + p[1] for p in per)
+    script_b = prepared_script_bytes(B)
+    bytes_per_cycle = script_b + sum(p[1] for p in per)
     return dict(dev_ms=dev_ms, e2e_ms=e2e_ms, cycles_per_step=W, streams=streams,
                 clocks=ck.summary(), bytes_per_cycle=bytes_per_cycle,
-                script_bytes=sum(p[0] for p in per), kernel_ms=dev_ms / args.steps,
+                script_bytes=script_b, kernel_ms=dev_ms / args.steps,
                 h2d=stim_pin.numel() * 4, d2h=wave_pin.numel() * 4, launches_per_step=2,
                 design=dict(designs=len(scripts), ands=ands, sizes=sizes.tolist(),
                             partitions=int(sum(s.num_partitions for s in scripts)),
@@ -882,8 +935,9 @@ def main():
                     help="timed: event records per window")
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
-    ap.add_argument("--per-item", type=int, default=2, choices=[2, 8],
-                    help="batched: lane words per work item (2: lane pairs, 8: octets)")
+    ap.add_argument("--per-item", type=int, default=8, choices=[2, 8],
+                    help="batched and timed: lane words per work item (8: octets, the "
+                         "default; 2: lane pairs)")
     ap.add_argument("--blocks", type=int, default=148, help="batched: script blocks")
     ap.add_argument("--cpu-cycles", type=int, default=160,
                     help="CPU baseline sample: cycles of one stream (about 10 s single-threaded)")

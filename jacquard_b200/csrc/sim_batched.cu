@@ -240,6 +240,18 @@ __device__ __forceinline__ uint32_t chunk_bytes(const Shared &sh, uint32_t k) {
   return b ? b : CHUNK_BYTES;
 }
 
+// Word offset of the flag words (a uint4 per 32 entries) in a prepared
+// SRAM/duplicate or clock-enable chunk of nq entries: right after the entries
+// in the compact form (metadata word 10 bit 0; the chunk is copied only that
+// far), at word 4096 otherwise.
+__host__ __device__ __forceinline__ uint32_t perm_flag_off(uint32_t nq) {
+  return ((nq >> 1) + 3) & ~3u;
+}
+__device__ __forceinline__ const uint4 *perm_flags(const Shared &sh, const uint32_t *C,
+                                                   uint32_t nq) {
+  return reinterpret_cast<const uint4 *>(C + ((sh.meta[10] & 1u) ? perm_flag_off(nq) : 4096u));
+}
+
 // Grid barrier between major stages, split in two so a CTA can load its
 // next item's script data between arriving and waiting.  The arrival count
 // is 64-bit and monotonic within a launch (the target grows by the grid each
@@ -661,8 +673,8 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
         // ---------------- SRAM & duplicate permutation + SRAM ports
         JQ_FAIL_IF(!ok)  // hooks done, chunk landed
         uint2 *St = Sb0;  // staging (the last stage's hooks are done)
-        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
+        const uint4 *F4 = perm_flags(sh, C, nq);
         for (uint32_t q = t; q < nq; q += BT) {
           const uint2 w = WO[perm_lin(C, q)];
           const uint4 fl = F4[q >> 5];
@@ -711,8 +723,8 @@ __device__ void run_item(const BatchParams &P, Shared &sh, uint2 *S, uint2 *WO, 
           next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
           have_next = true;
         }
-        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
+        const uint4 *F4 = perm_flags(sh, C, nq);
         // the old word is loaded only by warps where some stream of their
         // state word keeps its value (clock enable clear): none, when every
         // enable is set
@@ -1066,8 +1078,8 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
         // ---------------- SRAM & duplicate permutation + SRAM ports
         JQ_FAIL_IF(!ok)
         uint4 *St = S;
-        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
+        const uint4 *F4 = perm_flags(sh, C, nq);
         for (uint32_t q = t; q < nq; q += BT) {
           const uint4 w = WO[perm_lin(C, q)];
           const uint4 fl = F4[q >> 5];
@@ -1120,8 +1132,8 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
           next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
           have_next = true;
         }
-        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
+        const uint4 *F4 = perm_flags(sh, C, nq);
         // The new words come from shared memory; the old words (kept by
         // streams whose clock enable is clear) are loaded only by warps where
         // some stream of their state word keeps its value -- none, when
@@ -1357,7 +1369,7 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
         const uint32_t st0 = (reg_end + 31) & ~31u;
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
         const uint32_t ro = st0 + nq;
-        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
+        const uint4 *F4 = perm_flags(sh, C, nq);
         for (uint32_t q = el; q < nq; q += 128) {
           const uint32_t p = perm_lin(C, q);
           const uint4 w = S[4 * (wo_map[p >> 5] + (p & 31u)) + k];
@@ -1408,8 +1420,8 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
           next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
           have_next = true;
         }
-        const uint4 *F4 = reinterpret_cast<const uint4 *>(C + 4096);
         const uint32_t nq = num_ios * 32;
+        const uint4 *F4 = perm_flags(sh, C, nq);
         for (uint32_t q = el; q < nq; q += 128) {  // warp-uniform bound
           const uint32_t p = perm_lin(C, q);
           const uint4 src = S[4 * (wo_map[p >> 5] + (p & 31u)) + k];
@@ -2246,15 +2258,27 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
                              : 0xffffffffu;
       }
     }
-    if (t == 0) {
-      dst[off + 10] = compact ? 1u : 0u;
-      if (compact) dst[off + 11 + ns] = dst[off + 12 + ns] = 0;  // SRAM, commit: whole
-    }
+    if (t == 0) dst[off + 10] = compact ? 1u : 0u;
+    // SRAM/duplicate and clock-enable chunks: shuffle entries in q order, two
+    // per word.  In the compact form only the nq entries the kernel reads are
+    // kept, followed by their flag words (perm_flag_off), and the chunk's copy
+    // size (metadata word 11 + ci) ends there; otherwise all 8192 entries,
+    // flags at word 4096 as in the script.
     for (uint32_t ci = ns; ci < ns + 2; ++ci) {
       const uint32_t *C = ch + (size_t)ci * STAGE_WORDS;
       uint32_t *D = dch + (size_t)ci * STAGE_WORDS;
-      for (uint32_t q2 = t; q2 < 4096; q2 += BT)
+      const uint32_t nq = ci == ns ? (src[off + 4] * 4 + src[off + 7]) * 32 : nio * 32;
+      const uint32_t n2 = compact ? nq / 2 : 4096;
+      for (uint32_t q2 = t; q2 < n2; q2 += BT)
         D[q2] = perm_src(C, 2 * q2) | (perm_src(C, 2 * q2 + 1) << 16);
+      if (compact) {
+        const uint32_t fo = perm_flag_off(nq), nf = 4 * (nq / 32);
+        for (uint32_t i = t; i < nf; i += BT) D[fo + i] = C[4096 + i];
+        if (t == 0) {
+          const uint32_t bytes = (fo + nf) * 4;
+          dst[off + 11 + ci] = bytes < 16 ? 16u : bytes;
+        }
+      }
     }
     __syncthreads();  // shared state read before the next partition reuses it
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);

@@ -46,11 +46,16 @@ def test_summary_records_learned_vs_heuristic():
 def test_benchmark_uses_the_learned_cut_only_when_it_wins():
     """bench.py's default (--learned auto) takes the learned cut exactly when
     the committed summary shows it winning, bit-exact, on the benchmark's own
-    design."""
+    design in the configuration it runs (partitions per major stage, lane
+    words per work item)."""
     import bench
     with open(os.path.join(TRAINED, "costmodel.json")) as f:
         ev = json.load(f)["eval_soc2m"]
-    assert bench.learned_wins() == (ev["bit_exact_vs_heuristic"] and ev["gain"] > 1.0)
+    wins = ev["bit_exact_vs_heuristic"] and ev["gain"] > 1.0
+    cfg = (ev["parts_per_stage"], ev.get("lanes_per_item", 2))
+    assert bench.learned_wins(*cfg) == wins
+    other = (148, 8) if cfg != (148, 8) else (37, 2)
+    assert bench.learned_wins(*other) is False
 
 
 def test_model_predicts_larger_partitions_cost_more():

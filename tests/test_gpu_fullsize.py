@@ -58,7 +58,7 @@ def stream_of(rec, k):
     return (bits << torch.arange(32, device=rec.device)).sum(-1)
 
 
-def check_256_streams(d, s, packed, cycles, po_sig=None):
+def check_256_streams(d, s, packed, cycles, po_sig=None, per_item=0):
     """The batched interpreter over 256 streams (per-stream packed inputs
     `packed[k]`, (cycles+1, rio)) against the plain interpreter stream by
     stream: every snapshot (values and X) and the SRAM contents of every
@@ -69,7 +69,7 @@ def check_256_streams(d, s, packed, cycles, po_sig=None):
     streams = 32 * LANES
     tmpl = state.xmask_template(s)
     x0 = state.xmask_all_state_x(s)
-    B = batched.BatchedSim(s, LANES, record=True, po_signals=po_sig)
+    B = batched.BatchedSim(s, LANES, record=True, po_signals=po_sig, lanes_per_item=per_item)
     words = batched.input_words(s)
     stim = batched.to_batched(np.stack([p[:, :words] for p in packed]))  # (C+1, lanes, in_sigs)
     snap0 = np.zeros((LANES, B.sig), np.uint32)
@@ -130,23 +130,23 @@ def test_batched_256_streams_match_plain_and_oracle(soc):
 
 def test_benchmark_script_and_stimulus_256_streams_64_cycles():
     """The exact configuration bench.py times: its design, its script
-    (148 blocks, balanced partitions, at most 37 per major stage, flat stages
-    in the compact form, the cut bench.py picks), its stimulus (16 reset cycles, then p_toggle 0.25,
-    stream k seeded 1000 + k) and one of its 64-cycle windows with the
-    output waveform, 256 streams: every snapshot of every stream against the
-    plain interpreter, two streams against the oracle."""
+    (148 blocks, balanced partitions, at most 148 per major stage, flat
+    stages in the compact form, the cut bench.py picks), octet work items,
+    its stimulus (16 reset cycles, then p_toggle 0.25, stream k seeded
+    1000 + k) and one of its 64-cycle windows with the output waveform, 256
+    streams: every snapshot of every stream against the plain interpreter,
+    two streams against the oracle."""
     import bench
     d = bench.build_design()
-    model = bench.learned_model() if bench.learned_wins() else None  # as bench.py decides
-    s = bench.build_script(d, 148, target_parts=37, cost_model=model)
-    assert s.num_partitions <= 740
+    s, per_item = bench.default_batched_script(d)  # as bench.py builds it
+    assert per_item == 8 and s.num_partitions <= 148 * s.num_major_stages
     assert int(s.features[:, 14].max()) <= 1  # flat stages: the compact form
     cycles = 64
     packed = []
     for k in range(32 * LANES):
         vals = state.stimulus_inputs(s, d, cycles, 1000 + k, bench.P_TOGGLE, bench.RESET_CYCLES)
         packed.append(state.pack_inputs(s, vals))
-    check_256_streams(d, s, packed, cycles, po_sig=state.po_positions(s, d))
+    check_256_streams(d, s, packed, cycles, po_sig=state.po_positions(s, d), per_item=per_item)
 
 
 def test_timed_path_full_size_matches_oracle(soc):

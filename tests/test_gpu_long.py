@@ -123,8 +123,7 @@ class LaneStimulus:
 def test_soc_100k_cycles_256_streams_windowed():
     import bench
     d = bench.build_design()
-    model = bench.learned_model() if bench.learned_wins() else None  # as bench.py decides
-    s = bench.build_script(d, 148, target_parts=37, cost_model=model)
+    s, per_item = bench.default_batched_script(d)  # as bench.py builds it
     lanes, W, total = 8, 2000, 100_000 + bench.RESET_CYCLES
     total -= total % W  # whole windows: 100,000 cycles
     streams = 32 * lanes
@@ -134,7 +133,7 @@ def test_soc_100k_cycles_256_streams_windowed():
     x0 = state.xmask_all_state_x(s)
     po = state.po_positions(s, d)
     gen = LaneStimulus(s, d, lanes, seed=2024, reset=bench.RESET_CYCLES)
-    B = batched.BatchedSim(s, lanes, po_signals=po)
+    B = batched.BatchedSim(s, lanes, po_signals=po, lanes_per_item=per_item)
     checked = (streams - 1,)
     oracle_windows = {0, total // W // 2, total // W - 1}
     # snapshot 0 of the batched state and of the checked plain streams
