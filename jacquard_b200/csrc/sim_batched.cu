@@ -1191,12 +1191,19 @@ __device__ void run_item2(const BatchParams &P, Shared &sh, uint4 *S, uint4 *WO,
 #undef JQ_FAIL_IF
 #undef JQ_HOOKS_COMPACT
 
-// Shared memory of an octet item besides the chunks and tree slots: the
-// writeout map (writeout slot -> its first tree slot) and, for setup/hold
-// checks, the OR of each writeout word's clock enables per lane word.
-constexpr uint32_t OCT_AUX_WORDS = 256 + 256 * 8;
+// Script chunk of an octet item's ci-th copy: the boomerang stages, the
+// SRAM/duplicate chunk when the partition has one, the clock-enable chunk.
+__device__ __forceinline__ uint32_t oct_chunk(uint32_t ci, uint32_t ns, bool has_sram) {
+  return (!has_sram && ci == ns) ? ns + 1 : ci;
+}
+
 // Global-read slots an octet item loads (16 rounds of 128 slots).
 constexpr uint32_t OCT_MAX_GR = 2048;
+// Shared memory of an octet item besides the chunks and tree slots: the
+// writeout map (writeout slot -> its first tree slot), for setup/hold checks
+// the OR of each writeout word's clock enables per lane word, and the
+// partition's global-read source row.
+constexpr uint32_t OCT_AUX_WORDS = 256 + 256 * 8 + OCT_MAX_GR;
 
 // An octet work item: the block's partition list for 8 lane words (256
 // streams) at once, in the octet state layout, so every state access moves a
@@ -1220,6 +1227,7 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
   const uint32_t k = t & 3u, el = (uint32_t)t >> 2;
   uint32_t *const wo_map = aux;
   uint32_t *const clk_or = aux + 256;
+  uint32_t *const gr_src = aux + 256 + 256 * 8;
   // the octet's words: signal s (value plane) at 16 * (og * V + s)
   const size_t grp_base = ((size_t)og * P.vsig) << 4;
   size_t off = 0;
@@ -1228,12 +1236,12 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
     __syncthreads();
     long long t_start = clock64();
     if (t < 256) sh.meta[t] = __ldg(script + off + t);
-    uint32_t e[16];  // global-read source of slot el + 128 m
-    {
-      const uint32_t *src = P.gr_sources + (size_t)pid * 8192;
-#pragma unroll
-      for (int m = 0; m < 16; ++m) e[m] = __ldg(src + el + 128 * m);
-    }
+    // the global-read sources of slots 0..OCT_MAX_GR-1 into shared memory
+    // (16 bytes per thread; the previous item's readers are done)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(gr_src + 4 * t)),
+                 "l"(P.gr_sources + (size_t)pid * 8192 + 4 * t)
+                 : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
     __syncthreads();
     const uint32_t ns = sh.meta[0];
     if (!ns) break;
@@ -1245,10 +1253,24 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
     const uint32_t *ch0 = script + off + 256 + 512 * (size_t)R;
     const bool has_sram = (num_srams | num_dup) != 0;
     const uint32_t nchunks = ns + (has_sram ? 2 : 1);
-    if (t == 0) {
-      const uint32_t nb = chunk_bytes(sh, 0);
-      mbar_expect_tx(&sh.bar[0], nb);
-      tma_load_1d(chunks, ch0, nb, &sh.bar[0]);
+    // a partition the octet form cannot run (the host checks the whole
+    // script before choosing this form, so only a malformed launch has one)
+    const bool runnable = need <= P.slot_cap && (sh.meta[10] & 1u);
+    // Every chunk of the partition at once, packed in order into the chunk
+    // buffers (the prepare step admits a partition to the octet form only
+    // when they fit): script data, never written, so the copies run during
+    // the grid-barrier wait below.
+    if (t == 0 && runnable) {
+      uint32_t total = 0;
+      for (uint32_t ci = 0; ci < nchunks; ++ci) total += chunk_bytes(sh, oct_chunk(ci, ns, has_sram));
+      mbar_expect_tx(&sh.bar[0], total);
+      uint32_t o = 0;
+      for (uint32_t ci = 0; ci < nchunks; ++ci) {
+        const uint32_t kc = oct_chunk(ci, ns, has_sram), nb = chunk_bytes(sh, kc);
+        tma_load_1d(reinterpret_cast<uint8_t *>(chunks) + o, ch0 + (size_t)STAGE_WORDS * kc, nb,
+                    &sh.bar[0]);
+        o += nb;
+      }
     }
     // the deferred wait of the grid barrier ending the previous major stage
     // (see run_item2); the waiting warps prefetch the commit rows
@@ -1260,31 +1282,29 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
             for (uint32_t l = i0; l < nl; l += n) prefetch_l2(rows + 32 * (size_t)l);
           })) {
         failed = true;
-        if (t == 0) mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if (t == 0 && runnable) mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout);
         return;
       }
       t_start = clock64();
     }
-    // a partition the octet form cannot run (the host checks the whole
-    // script before choosing this form, so only a malformed launch gets here)
-    if (need > P.slot_cap || !(sh.meta[10] & 1u)) {
-      if (t == 0) {
-        atomicCAS(&g_status[P.slot], 0, JQ_ERR_INVALID_ARG);
-        mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout);
-      }
-      ++uses0;
+    if (!runnable) {
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      if (t == 0) atomicCAS(&g_status[P.slot], 0, JQ_ERR_INVALID_ARG);
       failed = true;
       return;
     }
     if (P.constraints)
       for (uint32_t i = t; i < num_ios * 8; i += BT) clk_or[i] = 0;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();  // the source row landed
     // ---- global read: slot el + 128 m, its 16-byte part k, into tree slot
     // sw(slot) (the prepared stage-0 entries name the swizzled slot, which
     // stays within the slot's 32-aligned block)
     if (is_x) {
 #pragma unroll
       for (int m = 0; m < 16; ++m) {
-        const uint32_t ek = e[m];
+        const uint32_t ek = gr_src[el + 128 * m];
         uint4 *dst = &S[4 * sw(el + 128 * m) + k];
         if (ek < GR_SKIP) {
           const uint32_t *bp = (ek >> 31) ? out : in;
@@ -1302,7 +1322,7 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
         uint4 v[8];
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
-          const uint32_t ek = e[8 * h + m];
+          const uint32_t ek = gr_src[el + 128 * (8 * h + m)];
           v[m] = make_uint4(0, 0, 0, 0);
           if (ek < GR_SKIP) {
             const uint32_t *bp = (ek >> 31) ? out : in;
@@ -1313,7 +1333,7 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
         }
 #pragma unroll
         for (int m = 0; m < 8; ++m)
-          if (e[8 * h + m] != GR_SKIP) S[4 * sw(el + 128 * (8 * h + m)) + k] = v[m];
+          if (gr_src[el + 128 * (8 * h + m)] != GR_SKIP) S[4 * sw(el + 128 * (8 * h + m)) + k] = v[m];
       }
     }
     // writeout slot t's hook (stage << 8 | 32-slot block of the stage's
@@ -1323,49 +1343,39 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
       const uint32_t hw = sh.meta[128 + t / 2];
       my_hook = (t & 1) ? (hw >> 16) : (hw & 0xffffu);
     }
-    uint32_t reg_end = 0;  // end of the last stage region
-    for (uint32_t ci = 0; ci < nchunks; ++ci) {
-      const uint32_t b = ci & 1;
-      uint32_t *C = chunks + b * STAGE_WORDS;
-      if (ci == 0) __syncthreads();  // global read complete
-      if (t == 0 && ci + 1 < nchunks) {
-        const uint32_t nxt = (!has_sram && ci + 1 == ns) ? ns + 1 : ci + 1;
-        const uint32_t nb = chunk_bytes(sh, nxt);
-        mbar_expect_tx(&sh.bar[b ^ 1], nb);
-        tma_load_1d(chunks + (b ^ 1) * STAGE_WORDS, ch0 + (size_t)STAGE_WORDS * nxt, nb,
-                    &sh.bar[b ^ 1]);
+    // the chunks landed (a chunk that never arrives fails the item after a
+    // bounded wait; nothing is left in flight then) and the global read is
+    // complete
+    {
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout));
+      ++uses0;
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        return;
       }
-      uint32_t &uses = b ? uses1 : uses0;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[b], uses & 1u, P.chunk_timeout));
-      ++uses;
-#define JQ_FAIL_IF(cond)                                                    \
-  if (__syncthreads_or(cond)) {                                             \
-    failed = true;                                                          \
-    if (t == 0 && ci + 1 < nchunks)                                         \
-      mbar_wait(&sh.bar[b ^ 1], (b ? uses0 : uses1) & 1u, P.chunk_timeout); \
-    return;                                                                 \
-  }
+    }
+    uint32_t reg_end = 0;  // end of the last stage region
+    const uint32_t *C = chunks;
+    for (uint32_t ci = 0; ci < nchunks; ++ci) {
+      if (ci) C += chunk_bytes(sh, oct_chunk(ci - 1, ns, has_sram)) / 4;
       if (ci < ns) {
         // ---------------- compact stage ci: entries el + 128 m; its region
         // follows the previous one, so nothing it reads is overwritten
-        const uint32_t n = ok ? C[0] : 0u, base = ok ? C[1] : 0u;
-        if (ok) {
-          if ((my_hook >> 8) == ci) wo_map[t] = base + 32 * (my_hook & 255u);
-          for (uint32_t i = el; i < n; i += 128) {
-            const uint32_t en = C[4 + i];
-            const uint4 ga = ((en >> 29) & 1u) ? make_uint4(0, 0, 0, 0) : S[4 * (en & 8191u) + k];
-            const uint4 gb =
-                ((en >> 30) & 1u) ? make_uint4(0, 0, 0, 0) : S[4 * ((en >> 13) & 8191u) + k];
-            S[4 * (base + i) + k] = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u),
-                                          0u - ((en >> 28) & 1u));
-          }
-          reg_end = base + n;
+        const uint32_t n = C[0], base = C[1];
+        if ((my_hook >> 8) == ci) wo_map[t] = base + 32 * (my_hook & 255u);
+        for (uint32_t i = el; i < n; i += 128) {
+          const uint32_t en = C[4 + i];
+          const uint4 ga = ((en >> 29) & 1u) ? make_uint4(0, 0, 0, 0) : S[4 * (en & 8191u) + k];
+          const uint4 gb =
+              ((en >> 30) & 1u) ? make_uint4(0, 0, 0, 0) : S[4 * ((en >> 13) & 8191u) + k];
+          S[4 * (base + i) + k] = xand2(ga, gb, 0u - ((en >> 26) & 1u), 0u - ((en >> 27) & 1u),
+                                        0u - ((en >> 28) & 1u));
         }
-        JQ_FAIL_IF(!ok)
+        reg_end = base + n;
+        __syncthreads();
       } else if (has_sram && ci == ns) {
         // ---------------- SRAM & duplicate permutation + SRAM ports: staged
         // words past the last region, then 32 read-out slots per SRAM
-        JQ_FAIL_IF(!ok)
         const uint32_t st0 = (reg_end + 31) & ~31u;
         const uint32_t nq = (num_srams * 4 + num_dup) * 32;
         const uint32_t ro = st0 + nq;
@@ -1414,8 +1424,8 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
         __syncthreads();
       } else {
         // ---------------- clock-enable permutation and commit: signal el +
-        // 128 m, lane pair k; a warp's 8 signals lie in one state word
-        JQ_FAIL_IF(!ok)
+        // 128 m, lane pair k; a warp's 8 signals lie in one state word (two
+        // signals per thread per round measured 1% slower)
         if (t == 0 && is_last && sh.dyn) {
           next_ticket = atomicAdd(&g_bticket[P.slot], 1ull);
           have_next = true;
@@ -1467,7 +1477,6 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
           }
         }
       }
-#undef JQ_FAIL_IF
     }
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
     if (P.part_cycles) {
@@ -2279,6 +2288,15 @@ __global__ void __launch_bounds__(BT) jq_batched_prepare_kernel(
           dst[off + 11 + ci] = bytes < 16 ? 16u : bytes;
         }
       }
+    }
+    // an octet item copies all of a partition's chunks into its two chunk
+    // buffers at once: a partition whose copies do not fit is not admitted
+    if (t == 0 && compact && dst[off + 127] != 0xffffffffu) {
+      const bool sr = (src[off + 4] | src[off + 7]) != 0;
+      uint32_t total = dst[off + 12 + ns];  // clock-enable chunk
+      if (sr) total += dst[off + 11 + ns];
+      for (uint32_t ci = 0; ci < ns; ++ci) total += dst[off + 11 + ci];
+      if (total > 2 * CHUNK_BYTES) dst[off + 127] = 0xffffffffu;
     }
     __syncthreads();  // shared state read before the next partition reuses it
     off += 256 + 512 * (size_t)R + STAGE_WORDS * ((size_t)ns + 2);
