@@ -190,15 +190,19 @@ def build_design(seed=2, clusters=512, n_dff=200_000):
     return d
 
 
-MODEL_PATH = os.path.join(HERE, "jacquard_b200", "trained", "costmodel.npz")
+# Trained partition cost models (jacquard_b200/trained), one per work-item
+# form they were timed on: lane pairs and octets.
+MODEL_PATHS = {2: os.path.join(HERE, "jacquard_b200", "trained", "costmodel.npz"),
+               8: os.path.join(HERE, "jacquard_b200", "trained", "costmodel_octet.npz")}
 
 
-def learned_model():
-    """The trained partition cost model (jacquard_b200/trained), or None."""
-    if not os.path.exists(MODEL_PATH):
+def learned_model(per_item=2):
+    """The cost model trained on `per_item` work items, or None."""
+    p = MODEL_PATHS.get(per_item)
+    if p is None or not os.path.exists(p):
         return None
     from jacquard_b200 import costmodel
-    return costmodel.packed_from_file(MODEL_PATH)
+    return costmodel.packed_from_file(p)
 
 
 def learned_wins(parts_per_stage, lanes_per_item):
@@ -208,8 +212,11 @@ def learned_wins(parts_per_stage, lanes_per_item):
     words per work item), with the learned run bit-exact against the
     heuristic one.  The benchmark uses the learned cut by default only
     then."""
-    p = os.path.splitext(MODEL_PATH)[0] + ".json"
-    if not os.path.exists(MODEL_PATH) or not os.path.exists(p):
+    m = MODEL_PATHS.get(lanes_per_item)
+    if m is None:
+        return False
+    p = os.path.splitext(m)[0] + ".json"
+    if not os.path.exists(m) or not os.path.exists(p):
         return False
     with open(p) as f:
         ev = json.load(f).get("eval_soc2m", {})
@@ -218,28 +225,34 @@ def learned_wins(parts_per_stage, lanes_per_item):
             and ev.get("lanes_per_item", 2) == lanes_per_item)
 
 
-def default_batched_script(d, blocks=148, lanes=8, per_item=8, learned="auto"):
+def default_batched_script(d, blocks=148, lanes=8, per_item=8, learned="auto", split_every=4,
+                           input_weight16=0):
     """(script, lanes per item) exactly as the batched mode builds them with
     these options: balanced partitions, one round of work items per major
     stage, the learned cut when `learned` says so."""
     per_stage = blocks // max(1, lanes // per_item)
-    use = learned == "on" or (learned == "auto" and learned_wins(per_stage, per_item))
-    return build_script(d, blocks, cost_model=learned_model() if use else None,
-                        target_parts=per_stage), per_item
+    use = learned == "on" or (learned == "auto" and split_every == 4 and
+                              learned_wins(per_stage, per_item))
+    return build_script(d, blocks, cost_model=learned_model(per_item) if use else None,
+                        target_parts=per_stage, split_every=split_every,
+                        input_weight16=input_weight16), per_item
 
 
-def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0):
+def build_script(d, num_blocks, xprop=True, cost_model=None, target_parts=0, split_every=4,
+                 input_weight16=0):
     """target_parts > 0 cuts each major stage into at most that many
     partitions of balanced cone size in flat stages, without merges: the
     batched kernel then runs every stage as one round of work items, one per
-    CTA (a partition makes lanes / 2 lane-pair items); a cost model then
-    refines the cut (endpoints move off the partition predicted slowest).
-    Otherwise partitions come from the cone target, merged by the learned
-    rule when a model is given."""
-    return d.build_script(num_blocks=num_blocks, level_split=LEVEL_SPLIT, xprop=xprop,
+    CTA (a partition makes lanes / (lanes per item) items); a cost model then
+    chooses each stage's cut.  Otherwise partitions come from the cone
+    target, merged by the learned rule when a model is given.  Major stages
+    cover split_every logic levels each; without a model the balanced cut
+    weighs each chunk input as input_weight16 / 16 gates."""
+    split = LEVEL_SPLIT if split_every == 4 else tuple(range(split_every, 80, split_every))
+    return d.build_script(num_blocks=num_blocks, level_split=split, xprop=xprop,
                           target_cone=TARGET_CONE, cost_model=cost_model,
                           merge_passes=0 if target_parts else (3 if cost_model is not None else 1),
-                          target_parts=target_parts)
+                          target_parts=target_parts, input_weight16=input_weight16)
 
 
 def algorithmic_bytes_per_cycle(s, streams=1, arrivals=False, bit_sliced=False):
@@ -484,10 +497,11 @@ def run_mine_batched(args, rank, world):
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
     per_stage = args.blocks // max(1, args.lanes // args.per_item)  # one round of items
-    use_learned = args.learned == "on" or (args.learned == "auto" and
+    use_learned = args.learned == "on" or (args.learned == "auto" and args.split == 4 and
                                            learned_wins(per_stage, args.per_item))
-    model = learned_model() if use_learned else None
-    s, _ = default_batched_script(d, args.blocks, args.lanes, args.per_item, args.learned)
+    model = learned_model(args.per_item) if use_learned else None
+    s, _ = default_batched_script(d, args.blocks, args.lanes, args.per_item, args.learned,
+                                  args.split, args.input_weight16)
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
@@ -935,6 +949,10 @@ def main():
                     help="timed: event records per window")
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
+    ap.add_argument("--input-weight16", type=int, default=0,
+                    help="batched, heuristic cut: gates (x16) a chunk input weighs")
+    ap.add_argument("--split", type=int, default=4,
+                    help="batched: logic levels per major stage (the autotuner's split)")
     ap.add_argument("--per-item", type=int, default=8, choices=[2, 8],
                     help="batched and timed: lane words per work item (8: octets, the "
                          "default; 2: lane pairs)")

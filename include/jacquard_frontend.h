@@ -88,6 +88,10 @@ typedef struct {
    * CTA, so grid / groups partitions per stage keep every stage to one
    * round of items. */
   uint32_t target_parts;
+  /* Balanced mode without a cost model: a chunk's cost adds input_weight16 /
+   * 16 gates per distinct chunk input (the batched kernel's global read
+   * loads one slot per input); 0 counts gates and SRAMs only. */
+  uint32_t input_weight16;
 } jqf_build_params;
 
 #define JQF_FEATURES 24

@@ -208,6 +208,7 @@ void *jqf_build_script(void *dp, const jqf_build_params *bp, char *err, size_t e
     po.num_threads = bp->num_threads;
     po.merge_passes = bp->merge_passes;
     po.target_parts = bp->target_parts;
+    po.input_weight16 = bp->input_weight16;
     CostModel cm;
     std::vector<uint8_t> xp;
     if (bp->cost_model) {

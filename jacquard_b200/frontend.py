@@ -38,7 +38,8 @@ class _BuildParams(ctypes.Structure):
                 ("n_level_split", ctypes.c_uint32), ("level_split", c_u32p),
                 ("target_cone", ctypes.c_uint32), ("target_endpoint_bits", ctypes.c_uint32),
                 ("num_threads", ctypes.c_int32), ("merge_passes", ctypes.c_int32),
-                ("cost_model", ctypes.c_void_p), ("target_parts", ctypes.c_uint32)]
+                ("cost_model", ctypes.c_void_p), ("target_parts", ctypes.c_uint32),
+                ("input_weight16", ctypes.c_uint32)]
 
 
 class _ScriptInfo(ctypes.Structure):
@@ -206,12 +207,15 @@ class Design:
 
     def build_script(self, num_blocks=148, xprop=False, level_split=(), target_cone=0,
                      target_endpoint_bits=0, num_threads=0, merge_passes=1, cost_model=None,
-                     target_parts=0):
+                     target_parts=0, input_weight16=0):
         """cost_model: flat float32 array (JQF_COST_MODEL_FLOATS) or None.
         target_parts: when non-zero, each major stage is cut into at most
-        this many partitions of balanced cone size (target_cone unused)."""
+        this many partitions of balanced cone size (target_cone unused);
+        input_weight16 / 16 gates are then added per distinct chunk input
+        when no cost model chooses the cut."""
         return Script(self, num_blocks, xprop, level_split, target_cone,
-                      target_endpoint_bits, num_threads, merge_passes, cost_model, target_parts)
+                      target_endpoint_bits, num_threads, merge_passes, cost_model, target_parts,
+                      input_weight16)
 
 
 class Script:
@@ -219,7 +223,7 @@ class Script:
 
     def __init__(self, design, num_blocks, xprop, level_split, target_cone,
                  target_endpoint_bits, num_threads, merge_passes, cost_model=None,
-                 target_parts=0):
+                 target_parts=0, input_weight16=0):
         lib = _lib()
         ls = (ctypes.c_uint32 * max(1, len(level_split)))(*level_split)
         cm = None
@@ -228,7 +232,8 @@ class Script:
             assert cm.size == COST_MODEL_FLOATS
         bp = _BuildParams(num_blocks, int(bool(xprop)), len(level_split), ls, target_cone,
                           target_endpoint_bits, num_threads, merge_passes,
-                          cm.ctypes.data if cm is not None else None, target_parts)
+                          cm.ctypes.data if cm is not None else None, target_parts,
+                          input_weight16)
         err = ctypes.create_string_buffer(512)
         h = lib.jqf_build_script(design._h, ctypes.byref(bp), err, 512)
         if not h:

@@ -1,15 +1,16 @@
 """Train the partition cost model on timings measured by the simulator.
 
   python -m jacquard_b200.train_costmodel [--samples 20000] [--steps 2000]
-         [--out jacquard_b200/trained/costmodel.npz] [--eval-clusters 1024]
+         [--out jacquard_b200/trained/costmodel.npz] [--per-item 8]
 
 1. Builds scripts of seeded SoC-family designs (the SoC workload's generator at
    several sizes and seeds) with varied level splits and balanced partition
    counts per major stage.
-2. Runs each on the batched interpreter in lane-pair work items (the batched
-   workload's form) with per-partition timing (`part_cycles`, which leaves
-   out the grid-barrier wait) and records log(mean SM cycles per work item)
-   next to the partition's 24 features.
+2. Runs each on the batched interpreter in octet work items (8 lane words
+   per item, the batched workload's form; --per-item 2 for lane pairs) with
+   per-partition timing (`part_cycles`, which leaves out the grid-barrier
+   wait) and records log(mean SM cycles per work item) next to the
+   partition's 24 features.
 3. Trains the MLP with Adam (lr 1e-3, batch 512) on the GPU kernels.
 4. Evaluates on fresh designs: balanced partitions without and with the
    learned cut choice (each major stage is cut with several weights of a
@@ -36,9 +37,12 @@ def build(design, split_every, parts, blocks=148, cost_model=None):
                                xprop=True, cost_model=cost_model, merge_passes=0, target_parts=parts)
 
 
-def measure(design, split_every, parts, lanes=8, cycles=4, blocks=148):
+def measure(design, split_every, parts, lanes=8, cycles=4, blocks=148, per_item=8):
     s = build(design, split_every, parts, blocks)
-    B = batched.BatchedSim(s, lanes, lanes_per_item=2)
+    try:
+        B = batched.BatchedSim(s, lanes, lanes_per_item=per_item)
+    except ValueError as e:  # octet items do not fit this script
+        raise RuntimeError(str(e)) from e
     B.load_state(np.zeros((lanes, B.sig), np.uint32))
     B.reset_sram()
     pc = torch.zeros(s.num_partitions, dtype=torch.int64, device="cuda")
@@ -46,12 +50,12 @@ def measure(design, split_every, parts, lanes=8, cycles=4, blocks=148):
     B.run(None, cycles, part_cycles=pc)
     torch.cuda.synchronize()
     assert B.status() == 0
-    per_item = pc.cpu().numpy().astype(np.float64) / ((lanes // 2) * cycles)
-    ok = per_item > 0
-    return s.features[ok], np.log(per_item[ok]).astype(np.float32)
+    t_item = pc.cpu().numpy().astype(np.float64) / ((lanes // per_item) * cycles)
+    ok = t_item > 0
+    return s.features[ok], np.log(t_item[ok]).astype(np.float32)
 
 
-def collect(target, seed0=100, log=print):
+def collect(target, seed0=100, log=print, per_item=8):
     feats, ys = [], []
     rng = np.random.default_rng(seed0)
     n = 0
@@ -61,9 +65,9 @@ def collect(target, seed0=100, log=print):
         d = frontend.Design(frontend.soc_params(seed=seed0 + k, n_clusters=clusters,
                                                 n_dff=200_000 * clusters // 512, n_sram=4))
         split = int(rng.choice([3, 4, 5]))
-        parts = int(rng.choice([12, 18, 24, 30, 37]))
+        parts = int(rng.choice([37, 74, 111, 148] if per_item == 8 else [12, 18, 24, 30, 37]))
         try:
-            f, y = measure(d, split, parts)
+            f, y = measure(d, split, parts, per_item=per_item)
         except RuntimeError as e:
             log(f"  skip: {e}")
             k += 1
@@ -102,7 +106,7 @@ def _lane_stimulus(script, design, lanes, cycles, seed):
 
 
 def evaluate(model_packed, clusters=1024, cycles=5000, lanes=8, seed=4242, split=4, parts=74,
-             log=print):
+             log=print, per_item=8):
     """Balanced partitions without and with the learned cut choice on one
     fresh design: batched stimulus-cycles/s over `cycles` cycles (device
     time, one launch each), same random stimulus.  Both runs must end with
@@ -112,13 +116,13 @@ def evaluate(model_packed, clusters=1024, cycles=5000, lanes=8, seed=4242, split
     d = frontend.Design(frontend.soc_params(seed=seed, n_clusters=clusters,
                                             n_dff=200_000 * clusters // 512))
     out = {"design_ands": int(d.num_and), "cycles": cycles, "streams": 32 * lanes,
-           "split": split, "parts_per_stage": parts}
+           "split": split, "parts_per_stage": parts, "lanes_per_item": per_item}
     finals = {}
     for name, cm in (("heuristic", None), ("learned", model_packed)):
         t0 = time.perf_counter()
         s = build(d, split, parts, cost_model=cm)
         bt = time.perf_counter() - t0
-        B = batched.BatchedSim(s, lanes)
+        B = batched.BatchedSim(s, lanes, lanes_per_item=per_item)
         rows = _lane_stimulus(s, d, lanes, cycles, seed + 1)
         snap0 = np.zeros((lanes, B.sig), np.uint32)
         snap0[:, :B.in_sigs] = rows[0]
@@ -153,22 +157,38 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--out", default=os.path.join(HERE, "trained", "costmodel.npz"))
-    ap.add_argument("--eval-clusters", type=int, default=1024)
+    ap.add_argument("--out", default=None,
+                    help="model file (default: trained/costmodel_octet.npz for octet items, "
+                         "trained/costmodel.npz for lane pairs)")
+    ap.add_argument("--per-item", type=int, default=8, choices=[2, 8],
+                    help="lane words per work item timed and evaluated")
+    ap.add_argument("--eval-clusters", type=int, default=None,
+                    help="held-out design size (default: 512 clusters, 2.3M gates, for octet "
+                         "items; 1024 for lane pairs)")
     ap.add_argument("--eval-cycles", type=int, default=5000)
-    ap.add_argument("--eval-parts", type=int, default=74, help="partitions per major stage")
+    ap.add_argument("--eval-parts", type=int, default=None,
+                    help="partitions per major stage (default: one round of items)")
     ap.add_argument("--eval-only", action="store_true",
                     help="evaluate the model saved at --out (no collection or training)")
     args = ap.parse_args()
+    pi = args.per_item
+    if args.out is None:
+        args.out = os.path.join(HERE, "trained", "costmodel_octet.npz" if pi == 8 else "costmodel.npz")
+    # one round of items per major stage on 148 CTAs: 148 partitions of
+    # octet items, 37 of lane pairs (4 items each)
+    soc_parts = 148 if pi == 8 else 37
+    ev_clusters = args.eval_clusters or (512 if pi == 8 else 1024)
+    ev_parts = args.eval_parts or (148 if pi == 8 else 74)
     if args.eval_only:
         packed = costmodel.packed_from_file(args.out)
-        ev = evaluate(packed, clusters=args.eval_clusters, cycles=args.eval_cycles,
-                      parts=args.eval_parts)
-        ev_soc = evaluate(packed, clusters=512, cycles=args.eval_cycles, seed=2, parts=37)
+        ev = evaluate(packed, clusters=ev_clusters, cycles=args.eval_cycles, parts=ev_parts,
+                      per_item=pi)
+        ev_soc = evaluate(packed, clusters=512, cycles=args.eval_cycles, seed=2, parts=soc_parts,
+                          per_item=pi)
         print(json.dumps({"eval": ev, "eval_soc2m": ev_soc}))
         return
     t0 = time.time()
-    X, y = collect(args.samples)
+    X, y = collect(args.samples, per_item=pi)
     print(f"collected {len(y)} partitions in {time.time() - t0:.0f}s; log-cycles mean {y.mean():.2f} sd {y.std():.2f}")
     perm = np.random.default_rng(0).permutation(len(y))
     ntr = int(0.9 * len(y))
@@ -180,11 +200,13 @@ def main():
     base = float(np.var(y[te]))
     print(f"train loss {hist[0][1]:.3f} -> {hist[-1][1]:.3f}; held-out mse {mse:.4f} (variance {base:.4f}, R^2 {1 - mse / base:.3f})")
     m.save(args.out)
-    ev = evaluate(m.pack(), clusters=args.eval_clusters, cycles=args.eval_cycles,
-                  parts=args.eval_parts)
+    ev = evaluate(m.pack(), clusters=ev_clusters, cycles=args.eval_cycles, parts=ev_parts,
+                  per_item=pi)
     # the SoC workload's own design (2M gates, seed 2), one round of items
-    ev_soc = evaluate(m.pack(), clusters=512, cycles=args.eval_cycles, seed=2, parts=37)
-    summary = {"samples": int(len(y)), "steps": args.steps, "loss_start": hist[0][1],
+    ev_soc = evaluate(m.pack(), clusters=512, cycles=args.eval_cycles, seed=2, parts=soc_parts,
+                      per_item=pi)
+    summary = {"samples": int(len(y)), "steps": args.steps, "per_item": pi,
+               "loss_start": hist[0][1],
                "loss_end": hist[-1][1], "heldout_mse": mse, "heldout_var": base,
                "heldout_r2": 1 - mse / base, "eval": ev, "eval_soc2m": ev_soc}
     with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
