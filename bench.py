@@ -945,7 +945,7 @@ def main():
                     help="batched: 256 streams (default); plain: 1 stream; timed: 256 streams with "
                          "setup/hold checks and event drain; timed_plain: the same on one stream "
                          "(arrivals written); multi: 12 designs in one graph-captured launch")
-    ap.add_argument("--event-capacity", type=int, default=1 << 22,
+    ap.add_argument("--event-capacity", type=int, default=1 << 23,
                     help="timed: event records per window")
     ap.add_argument("--window", type=int, default=64)
     ap.add_argument("--lanes", type=int, default=8, help="batched: 32-stream lane words")
@@ -1028,7 +1028,10 @@ def main():
         if args.no_cpu or args.mode in ("timed", "timed_plain", "multi"):
             cpu_v, cpu_dt = None, 0.0
         else:
-            cpu_v, cpu_dt = cpu_baseline(r["script"], r["d"], cycles=args.cpu_cycles, threads=1)
+            # the reference's CPU path on the script form the reference arm
+            # runs (cone partitions, 148 blocks), one host thread
+            cpu_s = build_script(r["d"], 148) if args.mode == "batched" else r["script"]
+            cpu_v, cpu_dt = cpu_baseline(cpu_s, r["d"], cycles=args.cpu_cycles, threads=1)
         workload = WORKLOADS[args.mode]
         line = {"metric": METRIC, "value": mine_val, "unit": "stimulus-cycles/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
