@@ -887,7 +887,7 @@ def run_mine_multi(args, rank, world):
                 design=dict(designs=len(scripts), ands=ands, sizes=sizes.tolist(),
                             partitions=int(sum(s.num_partitions for s in scripts)),
                             script_mb_per_cycle=comb.script_words_per_cycle() * 4 / 1e6,
-                            lanes=lanes, graph=True),
+                            lanes=lanes, lanes_per_item=2, graph=True),
                 script=None, d=None)
 
 
@@ -967,8 +967,8 @@ def main():
                          "cut (auto: when its recorded gain on this design is above 1)")
     ap.add_argument("--no-check", action="store_true",
                     help="batched: skip the bit-exactness self-check of the timed windows")
-    ap.add_argument("--compare", action="store_true",
-                    help="also time the single-stream plain kernel on the same design")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="batched: skip timing the single-stream plain kernel on the same design")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -1057,8 +1057,12 @@ def main():
                 "clocks": r["clocks"]}
         if r.get("parity") is not None:
             line["parity"] = r["parity"]
-        if args.compare and args.mode == "batched":
+        if args.mode == "batched" and not args.no_compare:
+            # the single-stream plain interpreter on the same design: the
+            # metric's batched-against-plain ratio
             line["compare"] = compare_kernels(r["d"], args)
+            line["compare"]["batched_over_plain"] = \
+                mine_val / line["compare"]["plain_kernel"]["cycles_per_s"]
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
