@@ -789,13 +789,18 @@ def multi_design_sizes(n=12, lo=50_000, hi=4_000_000, seed=4):
     return np.exp(rng.uniform(np.log(lo), np.log(hi), size=n)).astype(np.int64)
 
 
+MULTI_OCTET_ANDS = 650  # gates per partition per major stage (multi mode, octet items)
+
+
 def run_mine_multi(args, rank, world):
     """Twelve designs of log-uniform size in [50k, 4M] AND nodes in one
     persistent launch (scripts relocated into one), replayed from a CUDA
     graph; 8 lane words (256 streams) per design, each stream with its own
     random stimulus (p_toggle 0.25), every design's primary outputs recorded
-    each cycle.  e2e: the stimulus copied in and the waveform copied out
-    around every replay."""
+    each cycle.  Octet items on balanced partitions of about
+    MULTI_OCTET_ANDS gates per major stage by default; each super stage's
+    items come from the ticket counter.  e2e: the stimulus copied in and the
+    waveform copied out around every replay."""
     import torch
     from jacquard_b200 import batched, state
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
@@ -807,14 +812,22 @@ def run_mine_multi(args, rank, world):
         d = build_design(seed=40 + 100 * rank + k, clusters=clusters,
                          n_dff=max(64, 200_000 * clusters // 512))
         ands += int(d.num_and)
-        scripts.append(build_script(d, 148))
+        if args.multi_per_item == 8:
+            # octet items: balanced partitions of about MULTI_OCTET_ANDS gates
+            # per major stage (several per block on large designs), so every
+            # partition fits an item's tree slots; items come from tickets
+            parts = max(1, -(-int(d.num_and) // (len(LEVEL_SPLIT) + 1) // MULTI_OCTET_ANDS))
+            scripts.append(build_script(d, 148, target_parts=parts))
+        else:
+            scripts.append(build_script(d, 148))
         designs.append(d)
     comb = batched.CombinedScript(scripts)
     lanes = args.lanes
     W = args.window
     po_sig = np.concatenate([[comb.signal(i, int(p)) for p in state.po_positions(s, d)]
                              for i, (s, d) in enumerate(zip(scripts, designs))]).astype(np.int64)
-    B = batched.BatchedSim(comb, lanes, device=dev, po_signals=po_sig)
+    B = batched.BatchedSim(comb, lanes, device=dev, po_signals=po_sig,
+                           lanes_per_item=args.multi_per_item)
     # stimulus: each design's input lane words, concatenated per lane
     rng = np.random.default_rng(4000 + rank)
     rows = np.zeros((W + 1, lanes, B.in_sigs), np.uint32)
@@ -887,7 +900,7 @@ def run_mine_multi(args, rank, world):
                 design=dict(designs=len(scripts), ands=ands, sizes=sizes.tolist(),
                             partitions=int(sum(s.num_partitions for s in scripts)),
                             script_mb_per_cycle=comb.script_words_per_cycle() * 4 / 1e6,
-                            lanes=lanes, lanes_per_item=2, graph=True),
+                            lanes=lanes, lanes_per_item=args.multi_per_item or 2, graph=True),
                 script=None, d=None)
 
 
@@ -953,6 +966,9 @@ def main():
                     help="batched, heuristic cut: gates (x16) a chunk input weighs")
     ap.add_argument("--split", type=int, default=4,
                     help="batched: logic levels per major stage (the autotuner's split)")
+    ap.add_argument("--multi-per-item", type=int, default=8, choices=[0, 8],
+                    help="multi: 8 runs octet items on balanced partitions (the default), "
+                         "0 lets the library pick (lane pairs on cone partitions)")
     ap.add_argument("--per-item", type=int, default=8, choices=[2, 8],
                     help="batched and timed: lane words per work item (8: octets, the "
                          "default; 2: lane pairs)")

@@ -180,19 +180,27 @@ def test_layout_roundtrip():
     assert np.array_equal(batched.from_batched(batched.to_batched(a), 5), a)
 
 
-def test_multi_design_single_launch_matches_oracle():
-    """Three designs of uneven size relocated into one script share one
-    persistent launch, captured in a CUDA graph and replayed; every snapshot
-    of every stream of every design equals the oracle's run of that design
-    and stream alone, and so do the SRAM contents."""
-    specs = [("tiny", 8, (5,)), ("sram", 16, (8,)), ("soc_mini", 148, (20, 40, 60))]
-    scripts = [cases.script(k, nb, sp, xprop=True) for k, nb, sp in specs]
-    lanes, cycles = 1, 8
+@pytest.mark.parametrize("per_item", [0, 8])
+def test_multi_design_single_launch_matches_oracle(per_item):
+    """Designs of uneven size relocated into one script share one persistent
+    launch, captured in a CUDA graph and replayed; every snapshot of every
+    checked stream of every design equals the oracle's run of that design
+    and stream alone, and so do the SRAM contents.  per_item 0: three
+    designs on one lane word (every stream checked); 8: octet items on
+    balanced partitions of two designs, 256 streams (every 17th checked)."""
+    if per_item == 8:
+        specs = [("sram", 16, (8,), 16), ("soc_mini", 148, SPLIT4, 37)]
+        lanes, step = 8, 17
+    else:
+        specs = [("tiny", 8, (5,), 0), ("sram", 16, (8,), 0), ("soc_mini", 148, (20, 40, 60), 0)]
+        lanes, step = 1, 1
+    scripts = [cases.script(k, nb, sp, xprop=True, target_parts=tp) for k, nb, sp, tp in specs]
+    cycles = 8
     S = 32 * lanes
     snaps = [np.stack([cases.stimulus(k, s, cycles, seed=500 + 37 * i + j, x_init=True)
-                       for j in range(S)]) for i, ((k, _, _), s) in enumerate(zip(specs, scripts))]
+                       for j in range(S)]) for i, ((k, _, _, _), s) in enumerate(zip(specs, scripts))]
     C = batched.CombinedScript(scripts)
-    BC = batched.BatchedSim(C, lanes, record=True)
+    BC = batched.BatchedSim(C, lanes, record=True, lanes_per_item=per_item)
     bts = [batched.to_batched(sn) for sn in snaps]  # (cycles+1, lanes, sig_d)
     snap0 = C.combine_states([bt[0] for bt in bts])
     assert snap0.shape == (lanes, BC.sig)
@@ -215,7 +223,7 @@ def test_multi_design_single_launch_matches_oracle():
         eff = snaps[d].shape[-1]
         got = batched.from_batched(C.design_state(d, got_all), eff)  # (S, cycles+1, eff)
         n_sram = max(1, s.sram_storage_size)
-        for k in range(S):
+        for k in range(0, S, step):
             want = snaps[d][k].reshape(-1).copy()
             osram = np.zeros(n_sram, np.uint32)
             osram_x = np.full(n_sram, 0xFFFFFFFF, np.uint32)
