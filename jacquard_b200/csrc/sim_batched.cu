@@ -1244,7 +1244,10 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
     asm volatile("cp.async.commit_group;" ::: "memory");
     __syncthreads();
     const uint32_t ns = sh.meta[0];
-    if (!ns) break;
+    if (!ns) {  // the list ended: nothing is left in flight
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      break;
+    }
     const uint32_t is_last = sh.meta[1], num_ios = sh.meta[2], io_off = sh.meta[3];
     const uint32_t num_srams = sh.meta[4], sram_off = sh.meta[5], R = sh.meta[6];
     const uint32_t num_dup = sh.meta[7];
@@ -1343,9 +1346,8 @@ __device__ void run_item8(const BatchParams &P, Shared &sh, uint4 *S, uint32_t *
       const uint32_t hw = sh.meta[128 + t / 2];
       my_hook = (t & 1) ? (hw >> 16) : (hw & 0xffffu);
     }
-    // the chunks landed (a chunk that never arrives fails the item after a
-    // bounded wait; nothing is left in flight then) and the global read is
-    // complete
+    // the chunks landed (copies that do not complete within the bounded
+    // wait fail the item and the launch) and the global read is complete
     {
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh.bar[0], uses0 & 1u, P.chunk_timeout));
       ++uses0;
