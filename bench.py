@@ -496,18 +496,27 @@ def run_mine_batched(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     d = build_design(seed=2 + rank, clusters=args.clusters, n_dff=200_000 * args.clusters // 512)
-    per_stage = args.blocks // max(1, args.lanes // args.per_item)  # one round of items
-    use_learned = args.learned == "on" or (args.learned == "auto" and args.split == 4 and
-                                           learned_wins(per_stage, args.per_item))
-    model = learned_model(args.per_item) if use_learned else None
-    s, _ = default_batched_script(d, args.blocks, args.lanes, args.per_item, args.learned,
-                                  args.split, args.input_weight16)
     lanes = args.lanes
     streams = 32 * lanes
     W = args.window
     assert W % 2 == 0, "even windows keep the final state in buffer A"
-    po_sig = state.po_positions(s, d)
-    B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig, lanes_per_item=args.per_item)
+    per_item = args.per_item
+    while True:
+        per_stage = args.blocks // max(1, args.lanes // per_item)  # one round of items
+        use_learned = args.learned == "on" or (args.learned == "auto" and args.split == 4 and
+                                               learned_wins(per_stage, per_item))
+        model = learned_model(per_item) if use_learned else None
+        s, _ = default_batched_script(d, args.blocks, args.lanes, per_item, args.learned,
+                                      args.split, args.input_weight16)
+        po_sig = state.po_positions(s, d)
+        try:
+            B = batched.BatchedSim(s, lanes, device=dev, po_signals=po_sig,
+                                   lanes_per_item=per_item)
+            break
+        except ValueError:
+            if per_item == 2:
+                raise
+            per_item = 2  # this design does not fit octet items: lane pairs
     # snapshot 0: inputs of cycle 0, every DFF/SRAM word X
     stim = batched_stimulus(s, d, streams, W, seed0=1000 + 7919 * rank)
     snap0 = np.zeros((lanes, B.sig), np.uint32)
@@ -571,7 +580,7 @@ def run_mine_batched(args, rank, world):
                             script_mb_per_cycle=format_b / 1e6,
                             script_read_mb_per_cycle=script_b / 1e6, rio=s.reg_io_state_size,
                             major_stages=s.num_major_stages, blocks=s.num_blocks, lanes=lanes,
-                            lanes_per_item=args.per_item,
+                            lanes_per_item=per_item,
                             partitioner="balanced: at most %d per major stage%s"
                             % (per_stage,
                                ", cut chosen by the learned cost model" if model is not None
