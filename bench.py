@@ -54,19 +54,31 @@ PROFILE_BATCHED = os.path.join(HERE, "profiles", "batched_kernel_soc2M_xprop.md"
 KERNEL_SRC = os.path.join(HERE, "jacquard_b200", "csrc", "sim_batched.cu")
 
 
+def kernel_code_hash(path=KERNEL_SRC):
+    """sha256 of a kernel source with its comments, trailing blanks and
+    empty lines removed: it changes with the code, not with comment edits."""
+    import hashlib
+    import re
+    with open(path) as f:
+        src = f.read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
+    lines = [ln.rstrip() for ln in src.splitlines() if ln.strip()]
+    return hashlib.sha256("\n".join(lines).encode()).hexdigest()
+
+
 def measured_traffic_per_cycle():
     """DRAM bytes (read + write) per simulated cycle of the 256-stream batched
     workload, from the ncu capture summarised in the kernel's profile (a
-    line `traffic_bytes_per_cycle: B source_sha256: H`), or None when that
-    capture was taken of another version of the kernel source."""
-    import hashlib
+    line `traffic_bytes_per_cycle: B source_sha256: H`, H the prefix of
+    kernel_code_hash of the captured source), or None when that capture was
+    taken of other kernel code."""
     import re
     try:
         with open(PROFILE_BATCHED) as f:
             m = re.search(r"traffic_bytes_per_cycle:\s*([0-9.eE+]+)\s+source_sha256:\s*([0-9a-f]+)",
                           f.read())
-        with open(KERNEL_SRC, "rb") as f:
-            h = hashlib.sha256(f.read()).hexdigest()
+        h = kernel_code_hash()
     except OSError:
         return None
     if not m or not h.startswith(m.group(2)):

@@ -3,18 +3,21 @@
 //
 // Layout: a lane word is one u32 holding one signal of 32 streams, where
 // `signal` is the bit position of the plain layout (word*32 + bit) and the X
-// plane of signal s is signal V + s.  The state interleaves lane pairs: the
-// (value, X) words of both lane words of a pair for one signal are one
-// 16-byte quad (phys() below), so a lane-pair work item reads or commits a
-// signal with one access.  In this form the boomerang 16-pair bit shuffle
+// plane of signal s is signal V + s.  The state interleaves lane groups: the
+// (value, X) words of a lane pair for one signal are one 16-byte quad, or
+// those of 8 lane words one 64-byte run (phys() below), so a work item reads
+// or commits a signal of its lane group with one access per 16 bytes of
+// adjacent threads.  In this form the boomerang 16-pair bit shuffle
 // becomes a word gather and every tree position evaluates one 32-stream word:
 //     v[p] = (v[p+L] ^ xa_p) & ((v[p+2L] ^ xb_p) | ob_p),  L = msb(p)
 // (the plain kernel's level-0 / shared / warp / bit-level tree steps are all
 // this one positional rule).  Semantics per stream are those of the plain
 // interpreter (csrc/kernel_v1_impl.cuh:32-563).
 //
-// Work item = (script block, lane pair or lane word) for one (cycle, major
-// stage).  When a major stage has no more items than CTAs, CTA i runs item i
+// Work item = (script block, lane word, lane pair or lane octet) for one
+// (cycle, major stage); octet items (run_item8) run compact partitions only,
+// with 64-byte tree slots and writeouts named in place.  When a major stage
+// has no more items than CTAs, CTA i runs item i
 // (a per-launch table in shared memory holds its script offset and first
 // partition); otherwise CTAs take items from a ticket counter.  Major stages
 // are separated by a split grid barrier: arrive after the last commit, wait
@@ -22,9 +25,9 @@
 // first rewritten by jq_batched_prepare (liveness of tree positions, a
 // thread-major tree form or a compact one-word-per-live-position form,
 // compacted global-read slots).  Each script chunk is staged into shared
-// memory with a TMA bulk copy (cp.async.bulk, mbarrier completion,
-// double-buffered one chunk ahead); the global read copies its slots with
-// cp.async.  Setup/hold checks run per stream in the commit: a word's arrival
+// memory with a TMA bulk copy (cp.async.bulk, mbarrier completion):
+// double-buffered one chunk ahead, or for octet items all of a partition's
+// chunks at once; the global read copies its slots with cp.async.  Setup/hold checks run per stream in the commit: a word's arrival
 // does not depend on the stream (it follows from the script's delays and
 // each script block's execution order), so the caller computes the arrival
 // tables once with the plain interpreter, and only the clock-enable gate of

@@ -45,3 +45,19 @@ def test_level_split_option():
     s4 = bench.build_script(d, 148, target_parts=37)
     s5 = bench.build_script(d, 148, target_parts=37, split_every=5)
     assert s4.num_major_stages == 20 and s5.num_major_stages == 16
+
+
+def test_traffic_figure_follows_code_not_comments(tmp_path):
+    """The recorded ncu traffic is reported while the kernel's code is the
+    captured one: comment and blank-line edits keep the hash, a code change
+    alters it."""
+    src = "// header\\nint f(int a) {  /* note */\\n  return a + 1;  // inc\\n}\\n"
+    a = tmp_path / "a.cu"
+    b = tmp_path / "b.cu"
+    c = tmp_path / "c.cu"
+    a.write_text(src)
+    b.write_text("// another header\n\n" + src.replace("// inc", "// increment"))
+    c.write_text(src.replace("a + 1", "a + 2"))
+    assert bench.kernel_code_hash(str(a)) == bench.kernel_code_hash(str(b))
+    assert bench.kernel_code_hash(str(a)) != bench.kernel_code_hash(str(c))
+    assert bench.measured_traffic_per_cycle() is not None  # the current kernel's capture
