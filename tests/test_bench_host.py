@@ -51,7 +51,7 @@ def test_traffic_figure_follows_code_not_comments(tmp_path):
     """The recorded ncu traffic is reported while the kernel's code is the
     captured one: comment and blank-line edits keep the hash, a code change
     alters it."""
-    src = "// header\\nint f(int a) {  /* note */\\n  return a + 1;  // inc\\n}\\n"
+    src = "// header\nint f(int a) {  /* note */\n  return a + 1;  // inc\n}\n"
     a = tmp_path / "a.cu"
     b = tmp_path / "b.cu"
     c = tmp_path / "c.cu"
