@@ -5,16 +5,20 @@ start, 16 reset cycles then p_toggle = 0.25 stimulus).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
                   [--mode batched|timed|plain|timed_plain|multi] [--lanes L]
-                  [--window C] [--learned auto|on|off] [--no-check]
+                  [--per-item 8|2] [--window C] [--learned auto|on|off]
+                  [--split S] [--no-check] [--no-compare]
 
 One step = one launch window of C cycles over all stimulus streams.  The
-batched mode partitions every major stage into blocks / (lanes / 2) balanced
-partitions (one round of lane-pair work items); with --learned the cost model
-chooses each stage's cut (auto: only when the committed training summary
-shows it winning, bit-exact, on this design).  `value` is device-timed
-throughput with inputs resident in HBM; `e2e` is the same through the C ABI
-with host buffers copied in and out inside the timed region; `parity` is the
-replay of two sampled streams of both timed regions on the plain interpreter.
+batched mode partitions every major stage into blocks / (lanes / per-item)
+balanced partitions: one round of work items, octet items (8 lane words,
+the default) or lane pairs.  With --learned the cost model trained on that
+item form chooses each stage's cut (auto: only when its committed training
+summary shows it winning, bit-exact, on this design in this configuration).
+`value` is device-timed throughput with inputs resident in HBM; `e2e` is the
+same through the C ABI with host buffers copied in and out inside the timed
+region; `parity` is the replay of two sampled streams of both timed regions
+on the plain interpreter; `compare` times the single-stream plain
+interpreter on the same design.
 --impl reference runs the reference's CPU interpreter path (this repository's
 C restatement of it, oracle/) on the host cores.  Multi-GPU: independent
 replicas (one design + its own stimulus streams per rank), weak scaling.
